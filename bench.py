@@ -1,0 +1,434 @@
+"""Template-matching benchmark: match-score Gtaps/s on one B200 (or N).
+
+Workload (one step): the five ImageProximity measures (SqrDistance,
+SqrDistance_Norm, AbsDistance, CrossCorr, CrossCorr_Norm) of a 4096x4096
+single-channel F32 image against a 31x31 F32 template cut from it. The
+image is a seeded sum of 200 isotropic Gaussian blobs (sigma uniform in
+4-40 px, amplitude uniform in 0-1) plus uniform noise in [0, 0.05]; the
+template is cut at a seeded offset. Taps are counted over the valid region
+((W-tw+1) x (H-th+1) x tw x th per measure); each call computes the full
+same-size map as the drop-in does.
+
+Timing: inputs resident on the device, the L2 flushed (256 MiB write, not
+timed) before every step, each step timed with CUDA events on the library's
+stream, K steps after W warm-up steps, max over ranks. `e2e` times the same
+step through the C ABI with host buffers in pinned memory: the source is
+sent each step and the five score maps read back.
+
+Ranks (torchrun, N>1): every rank runs its own copy of the workload on its
+own GPU (independent images; no collective on the data path), so the job's
+throughput is the sum of the ranks' taps over the slowest rank's time
+("scaling": "weak").
+
+--impl reference times the reference's own kernel source
+(cl-files/ImageProximity.cl, compiled for the host, oracle/_ref) on the host
+cores on a band of rows of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W_IMG, H_IMG, T_SIDE = 4096, 4096, 31
+MEASURES = ["SqrDistance", "SqrDistance_Norm", "AbsDistance", "CrossCorr", "CrossCorr_Norm"]
+METRIC = "match-score Gtaps/s, tensor vs plain FP32 on one B200, <=1e-5 rel err vs FP64"
+
+
+def blob_field(W, H, nblobs=200, seed=0):
+    """Seeded sum of isotropic Gaussian blobs plus uniform noise (float32)."""
+    rng = np.random.default_rng(seed)
+    img = np.zeros((H, W), np.float64)
+    xs = rng.uniform(0, W, nblobs)
+    ys = rng.uniform(0, H, nblobs)
+    sig = rng.uniform(4, 40, nblobs)
+    amp = rng.uniform(0, 1, nblobs)
+    for x, y, s, a in zip(xs, ys, sig, amp):
+        r = int(np.ceil(5 * s))
+        x0, x1 = max(0, int(x) - r), min(W, int(x) + r + 1)
+        y0, y1 = max(0, int(y) - r), min(H, int(y) + r + 1)
+        gx = np.exp(-0.5 * ((np.arange(x0, x1) - x) / s) ** 2)
+        gy = np.exp(-0.5 * ((np.arange(y0, y1) - y) / s) ** 2)
+        img[y0:y1, x0:x1] += a * np.outer(gy, gx)
+    img += rng.uniform(0, 0.05, (H, W))
+    return img.astype(np.float32)
+
+
+def workload(seed=0):
+    S = blob_field(W_IMG, H_IMG, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    ty = int(rng.integers(0, H_IMG - T_SIDE))
+    tx = int(rng.integers(0, W_IMG - T_SIDE))
+    T = S[ty:ty + T_SIDE, tx:tx + T_SIDE].copy()
+    return S, T
+
+
+def valid_taps(W, H, tw, th, nch=1):
+    return (W - tw + 1) * (H - th + 1) * tw * th * nch
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.path = os.path.join("/tmp", f"bench_clocks_{os.getpid()}.csv")
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def allreduce_max(x):
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized():
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_initialized():
+        dist.barrier()
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from openclipp_b200 import ocip
+
+    S, T = workload(seed=1234 + rank)
+    H, W = S.shape
+    taps_step = valid_taps(W, H, T_SIDE, T_SIDE) * len(MEASURES)
+
+    ctx = ocip.Context(local)
+    path = {"auto": ocip.PATH_AUTO, "plain": ocip.PATH_PLAIN, "tensor": ocip.PATH_TENSOR}[args.path]
+    ctx.set_path(path)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # Device-resident arm.
+    Si, Ti = ocip.Image(S), ocip.Image(T)
+    outs = [np.zeros((H, W), np.float32) for _ in MEASURES]
+    Ds = [ocip.Image(o) for o in outs]
+    Si.send()
+    Ti.send()
+
+    def step():
+        for m, D in zip(MEASURES, Ds):
+            ocip.check(ocip.proximity(m, Si, Ti, D), m)
+
+    per_kernel = {}
+
+    def timed_steps(n, record=False):
+        times = []
+        for _ in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if record:
+                # per-measure events for the roofline of the dominant kernel
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(MEASURES) + 1)]
+                ev[0].record(stream)
+                for i, (m, D) in enumerate(zip(MEASURES, Ds)):
+                    ocip.check(ocip.proximity(m, Si, Ti, D), m)
+                    ev[i + 1].record(stream)
+            else:
+                step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            if record:
+                for i, m in enumerate(MEASURES):
+                    per_kernel.setdefault(m, []).append(ev[i].elapsed_time(ev[i + 1]))
+        return times
+
+    timed_steps(args.warmup)
+    paths_used = {}
+    for m, D in zip(MEASURES, Ds):
+        ocip.check(ocip.proximity(m, Si, Ti, D), m)
+        paths_used[m] = {1: "plain", 2: "tensor"}[ctx.last_path()]
+    ctx.finish()
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = ocip.launch_count()
+    with Clocks(local) as clk:
+        times = timed_steps(args.steps, record=True)
+    launches = ocip.launch_count() - launches0
+    torch.cuda.synchronize()
+    barrier()
+    ms_step = allreduce_max(float(np.mean(times)))
+    clocks = clk.summary()
+
+    # Accuracy of this run's maps against an FP64 oracle on a crop.
+    errs = accuracy_report(S, T, outs, Ds) if rank == 0 else {}
+
+    # End-to-end arm: pinned host buffers, send + 5 calls + 5 reads per step.
+    e2e_ms = run_e2e(args, ocip, torch, ctx, S, T, stream)
+    e2e_ms = allreduce_max(e2e_ms)
+
+    value = taps_step * world / (ms_step * 1e-3) / 1e9
+    e2e_value = taps_step * world / (e2e_ms * 1e-3) / 1e9
+
+    # Roofline of the dominant kernel (largest share of the step).
+    med = {m: float(np.median(v)) for m, v in per_kernel.items()}
+    dom = max(med, key=med.get)
+    peaks = load_peaks()
+    taps_meas = valid_taps(W, H, T_SIDE, T_SIDE)
+    same_taps = W * H * T_SIDE * T_SIDE
+    tflops = 2.0 * same_taps / (med[dom] * 1e-3) / 1e12
+    roof = {"kernel": f"{dom} ({paths_used[dom]})", "bound": "tensor", "achieved": round(tflops, 2),
+            "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+            "frac": round(tflops / peaks["bf16_tflops"], 4), "traffic": None,
+            "peak_source": peaks["source"],
+            "flops_convention": "2 per tap (one multiply-add), same-size map "
+                                f"{W}x{H}x{T_SIDE}x{T_SIDE} per launch"}
+
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Gtaps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded blob field, template cut from it)",
+        "config": {"workload": f"{W}x{H} F32 1ch, {T_SIDE}x{T_SIDE} template, 5 measures per step",
+                   "path": args.path, "paths_used": paths_used,
+                   "taps_per_step": taps_step, "taps_counted": "valid region",
+                   "l2": "flushed before every step (256 MiB write, outside the timed events)"},
+        "per_measure_ms": {m: round(v, 4) for m, v in med.items()},
+        "per_measure_gtaps": {m: round(taps_meas / (v * 1e-3) / 1e9, 1) for m, v in med.items()},
+        "accuracy_vs_fp64": errs,
+        "roofline": roof,
+        "e2e": {"value": round(e2e_value, 2), "unit": "Gtaps/s",
+                "h2d_bytes_per_step": int(S.nbytes + T.nbytes),
+                "d2h_bytes_per_step": int(sum(o.nbytes for o in outs))},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(S, T, budget_s=args.cpu_seconds)
+    for D in Ds:
+        D.release()
+    Si.release()
+    Ti.release()
+    ctx.close()
+    return result
+
+
+def run_e2e(args, ocip, torch, ctx, S, T, stream):
+    H, W = S.shape
+    hS = torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy()
+    hS[:] = S
+    hT = torch.empty(T.shape, dtype=torch.float32, pin_memory=True).numpy()
+    hT[:] = T
+    houts = [torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy() for _ in MEASURES]
+    Si, Ti = ocip.Image(hS), ocip.Image(hT)
+    Ds = [ocip.Image(o) for o in houts]
+
+    def step():
+        Si.send()
+        Ti.send()
+        for m, D in zip(MEASURES, Ds):
+            ocip.check(ocip.proximity(m, Si, Ti, D), m)
+        for D in Ds:
+            D.read()
+
+    for _ in range(max(1, min(args.warmup, 3))):
+        step()
+    times = []
+    for _ in range(max(1, min(args.steps, 5))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    for D in Ds:
+        D.release()
+    Si.release()
+    Ti.release()
+    return float(np.mean(times))
+
+
+def accuracy_report(S, T, outs, Ds):
+    """Max abs / relative error of each map vs the FP64 oracle on a crop."""
+    from oracle import oracle as O
+    for D in Ds:
+        D.read()
+    y0, x0, n = 1000, 1000, 192
+    crop = S[y0 - 20:y0 + n + 20, x0 - 20:x0 + n + 20]
+    rep = {}
+    for i, m in enumerate(MEASURES):
+        ex = O.proximity_exact(i, crop, T)[20:-20, 20:-20]
+        got = outs[i][y0:y0 + n, x0:x0 + n].astype(np.float64)
+        scale = np.abs(ex).max()
+        rel = np.abs(got - ex) / np.maximum(np.abs(ex), 1e-300)
+        rep[m] = {"max_abs": float(np.abs(got - ex).max()), "max_rel": float(rel.max()),
+                  "max_abs_over_maxref": float(np.abs(got - ex).max() / scale)}
+    return rep
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "source": "measured (MEASURED_PEAKS.json, burst)"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def cpu_reference_time(S, T, rows):
+    """Seconds for the reference kernel source (host build, all threads) on
+    output rows [0, rows) for the five measures."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    for i in range(len(MEASURES)):
+        O.proximity_reference(i, S, T, rows=(0, rows))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(S, T, budget_s=15.0):
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"value": None, "unit": "Gtaps/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference kernels not built"}
+    rows = 8
+    dt = cpu_reference_time(S, T, rows)
+    rows = int(max(8, min(S.shape[0], rows * budget_s / max(dt, 1e-3))))
+    dt = cpu_reference_time(S, T, rows)
+    H, W = S.shape
+    taps = rows * (W - T_SIDE + 1) * T_SIDE * T_SIDE * len(MEASURES)
+    return {"value": round(taps / dt / 1e9, 4), "unit": "Gtaps/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())),
+            "kind": "reference",
+            "sample": f"output rows 0-{rows} of the {W}x{H} map, 5 measures, "
+                      f"cl-files/ImageProximity.cl built for the host (OpenMP), {dt:.1f} s"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref not built (no reference sources)"}
+    S, T = workload(seed=1234)
+    H, W = S.shape
+    rows = 4
+    dt = cpu_reference_time(S, T, rows)
+    budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    rows = int(max(4, min(H, rows * budget / max(dt, 1e-3))))
+    taps = rows * (W - T_SIDE + 1) * T_SIDE * T_SIDE * len(MEASURES)
+    for _ in range(args.warmup):
+        cpu_reference_time(S, T, max(1, rows // 8))
+    times = [cpu_reference_time(S, T, rows) for _ in range(args.steps)]
+    value = taps / float(np.mean(times)) / 1e9
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    sample = (f"output rows 0-{rows} of the {W}x{H} map per step, 5 measures, "
+              "cl-files/ImageProximity.cl built for the host (OpenMP)")
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Gtaps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(float(np.mean(times)) * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded blob field, template cut from it)",
+            "config": {"workload": f"{W}x{H} F32 1ch, {T_SIDE}x{T_SIDE} template, 5 measures per step",
+                       "taps_counted": "valid region"},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Gtaps/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "Gtaps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--path", choices=["auto", "tensor", "plain"], default="tensor")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, world, rank)
+        if res is not None:
+            print(json.dumps(res))
+        return
+    world, rank, local = dist_setup()
+    res = run_ours(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(res))
+    import torch.distributed as dist
+    if dist.is_initialized():
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

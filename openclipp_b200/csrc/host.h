@@ -1,0 +1,101 @@
+// Host-side objects behind the opaque ocip* handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <new>
+#include <string>
+
+#include "../../include/OpenCLIPP.h"
+#include "internal.h"
+
+namespace ocipb {
+
+// Error carried to the C boundary, where it becomes the return code.
+struct Error {
+  int code;
+  std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+const char* error_name(int code);
+
+// Counterpart of the reference's COpenCL (C++/OpenCL.cpp:48-69): one device
+// and one in-order queue (a CUDA stream), plus scratch buffers the kernels
+// reuse from call to call.
+struct Context {
+  enum ScratchSlot { kTemplateEnergy = 0, kWindowStats = 1, kTensorAux = 2, kNumScratch = 4 };
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  cudaStream_t stream = nullptr;
+  std::string name;
+  int path = 1;       // ocipProximityPath; PLAIN by default (the drop-in)
+  int last_path = 1;  // path that served the last proximity call
+  void* scratch(int slot, size_t bytes);
+  ~Context();
+
+ private:
+  struct Scratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+  };
+  Scratch scratch_[kNumScratch];
+};
+
+// Counterpart of the reference's Image (C++/Image.cpp:154-166) over a Buffer
+// (C++/Buffer.cpp): a device buffer plus the caller's host buffer, which the
+// image does not own.
+struct Image {
+  static constexpr uint32_t kMagic = 0x0C1F1A6Eu;
+  uint32_t magic = kMagic;
+  Context* ctx = nullptr;
+  SImage desc{};
+  void* host = nullptr;
+  void* dev = nullptr;
+  size_t pitch = 0;        // device row pitch, bytes (multiple of 128)
+  bool in_device = false;  // Memory::m_isInDevice (C++/Buffer.cpp:30-43)
+  size_t row_bytes() const {
+    return (size_t)desc.Width * desc.Channels * type_bytes((int)desc.Type);
+  }
+};
+
+// Program handle: the reference's MultiProgram subclasses that own temporary
+// buffers (Integral: C++/programs/Integral.cpp:42-95).
+struct Program {
+  static constexpr uint32_t kMagic = 0x0C1F9E0Au;
+  enum Kind { kIntegral = 1, kProximityFFT = 2 };
+  uint32_t magic = kMagic;
+  int kind = kIntegral;
+  Context* ctx = nullptr;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+extern thread_local std::string g_last_error;
+extern std::map<Context*, bool> g_contexts;
+extern Context* g_current;
+
+// Runs a C-ABI body, turning exceptions into the returned error code (the
+// reference's H() macro, OpenCLIPP/OpenCLIPP.cpp:82).
+#define OCIP_GUARD(...)                         \
+  try {                                         \
+    __VA_ARGS__;                                \
+  } catch (const ocipb::Error& err_) {          \
+    ocipb::g_last_error = err_.msg;             \
+    return err_.code;                           \
+  } catch (const std::bad_alloc&) {             \
+    ocipb::g_last_error = "out of host memory"; \
+    return CL_OUT_OF_HOST_MEMORY;               \
+  }                                             \
+  return CL_SUCCESS;
+
+Context& current();
+Image& image(ocipImage h);
+void send(Image& img);
+void send_if_needed(Image& img);
+DevImage dev_view(const Image& img);
+
+}  // namespace ocipb

@@ -1,0 +1,268 @@
+// ocip* processing entry points: ImageProximity and Integral.
+//
+// Argument checks keep the reference's order and codes:
+//   ImageProximity (C++/programs/ImageProximity.cpp:34-163): template larger
+//   than source -> CL_INVALID_VALUE; SameType(S, T) (Program.cpp:440-446)
+//   -> CL_INVALID_VALUE; CheckSameSize(S, D) -> CL_INVALID_IMAGE_SIZE;
+//   CheckSameNbChannels(S, D) -> CL_INVALID_VALUE; CheckFloat(D) ->
+//   CL_INVALID_VALUE.
+//   Integral (C++/programs/Integral.cpp:97-141, :143-146): Dest type F32 or
+//   F64 else CL_INVALID_VALUE, then CheckSameSize(S, D).
+// A handle that is not an image gives CL_INVALID_MEM_OBJECT (the reference
+// casts blindly), an image of another context CL_INVALID_CONTEXT.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/OpenCLIPP.h"
+#include "../../include/OpenCLIPP_B200.h"
+#include "host.h"
+#include "internal.h"
+#include "tensor.h"
+
+using namespace ocipb;
+
+namespace ocipb {
+
+const char* error_name(int code) {
+  switch (code) {
+    case 0: return "SUCCESS";
+    case -1: return "CL_DEVICE_NOT_FOUND";
+    case -2: return "CL_DEVICE_NOT_AVAILABLE";
+    case -3: return "CL_COMPILER_NOT_AVAILABLE";
+    case -4: return "CL_MEM_OBJECT_ALLOCATION_FAILURE";
+    case -5: return "CL_OUT_OF_RESOURCES";
+    case -6: return "CL_OUT_OF_HOST_MEMORY";
+    case -7: return "CL_PROFILING_INFO_NOT_AVAILABLE";
+    case -8: return "CL_MEM_COPY_OVERLAP";
+    case -9: return "CL_IMAGE_FORMAT_MISMATCH";
+    case -10: return "CL_IMAGE_FORMAT_NOT_SUPPORTED";
+    case -11: return "CL_BUILD_PROGRAM_FAILURE";
+    case -12: return "CL_MAP_FAILURE";
+    case -30: return "CL_INVALID_VALUE";
+    case -31: return "CL_INVALID_DEVICE_TYPE";
+    case -32: return "CL_INVALID_PLATFORM";
+    case -33: return "CL_INVALID_DEVICE";
+    case -34: return "CL_INVALID_CONTEXT";
+    case -35: return "CL_INVALID_QUEUE_PROPERTIES";
+    case -36: return "CL_INVALID_COMMAND_QUEUE";
+    case -37: return "CL_INVALID_HOST_PTR";
+    case -38: return "CL_INVALID_MEM_OBJECT";
+    case -39: return "CL_INVALID_IMAGE_FORMAT_DESCRIPTOR";
+    case -40: return "CL_INVALID_IMAGE_SIZE";
+    case -41: return "CL_INVALID_SAMPLER";
+    case -42: return "CL_INVALID_BINARY";
+    case -43: return "CL_INVALID_BUILD_OPTIONS";
+    case -44: return "CL_INVALID_PROGRAM";
+    case -45: return "CL_INVALID_PROGRAM_EXECUTABLE";
+    case -46: return "CL_INVALID_KERNEL_NAME";
+    case -47: return "CL_INVALID_KERNEL_DEFINITION";
+    case -48: return "CL_INVALID_KERNEL";
+    case -49: return "CL_INVALID_ARG_INDEX";
+    case -50: return "CL_INVALID_ARG_VALUE";
+    case -51: return "CL_INVALID_ARG_SIZE";
+    case -52: return "CL_INVALID_KERNEL_ARGS";
+    case -53: return "CL_INVALID_WORK_DIMENSION";
+    case -54: return "CL_INVALID_WORK_GROUP_SIZE";
+    case -55: return "CL_INVALID_WORK_ITEM_SIZE";
+    case -56: return "CL_INVALID_GLOBAL_OFFSET";
+    case -57: return "CL_INVALID_EVENT_WAIT_LIST";
+    case -58: return "CL_INVALID_EVENT";
+    case -59: return "CL_INVALID_OPERATION";
+    case -60: return "CL_INVALID_GL_OBJECT";
+    case -61: return "CL_INVALID_BUFFER_SIZE";
+    default: return "Unknown CL error";
+  }
+}
+
+namespace {
+
+void same_context(const Context& ctx, const Image& img) {
+  if (img.ctx != &ctx) fail(CL_INVALID_CONTEXT, "image belongs to another context");
+}
+
+bool same_type(const Image& a, const Image& b) {
+  return a.desc.Type == b.desc.Type && a.desc.Channels == b.desc.Channels;
+}
+
+void proximity_run(Context& ctx, Measure m, Image& S, Image& T, Image& D, int path) {
+  send_if_needed(S);
+  send_if_needed(T);
+  const DevImage s = dev_view(S), t = dev_view(T), d = dev_view(D);
+  cudaError_t e = cudaSuccess;
+  bool done = false;
+  if (path != OCIP_PATH_PLAIN && tensor_supports(m, s, t, d, path == OCIP_PATH_TENSOR)) {
+    e = launch_proximity_tensor(ctx, m, s, t, d);
+    done = true;
+    ctx.last_path = OCIP_PATH_TENSOR;
+  }
+  if (!done) {
+    void* tt = ctx.scratch(Context::kTemplateEnergy, 64);
+    e = launch_proximity_plain(m, s, t, d, tt, ctx.stream);
+    ctx.last_path = OCIP_PATH_PLAIN;
+  }
+  check_cuda(e, "proximity kernel launch");
+  D.in_device = true;
+}
+
+void proximity(Measure m, ocipImage hs, ocipImage ht, ocipImage hd) {
+  Context& ctx = current();
+  Image& S = image(hs);
+  Image& T = image(ht);
+  Image& D = image(hd);
+  same_context(ctx, S);
+  same_context(ctx, T);
+  same_context(ctx, D);
+  if (T.desc.Width > S.desc.Width || T.desc.Height > S.desc.Height)
+    fail(CL_INVALID_VALUE, "Template image must be smaller than the source image.");
+  if (!same_type(S, T)) fail(CL_INVALID_VALUE, "Source and Template must have same type.");
+  if (S.desc.Width != D.desc.Width || S.desc.Height != D.desc.Height)
+    fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  if (S.desc.Channels != D.desc.Channels)
+    fail(CL_INVALID_VALUE, "Different number of channels used");
+  if (!type_is_float((int)D.desc.Type))
+    fail(CL_INVALID_VALUE, "non-float image used when not allowed");
+  proximity_run(ctx, m, S, T, D, ctx.path);
+}
+
+// The FFT-named entry points (C++/programs/ImageProximityFFT.cpp:112-210)
+// check in their own order with their own codes, then compute the same
+// measure; here on the tensor path where it applies (no FFT).
+void proximity_fft(Measure m, ocipProgram hp, ocipImage hs, ocipImage ht, ocipImage hd) {
+  Context& ctx = current();
+  Program* prog = reinterpret_cast<Program*>(hp);
+  if (prog == nullptr || prog->magic != Program::kMagic || prog->kind != Program::kProximityFFT)
+    fail(CL_INVALID_PROGRAM, "invalid program handle");
+  Image& S = image(hs);
+  Image& T = image(ht);
+  Image& D = image(hd);
+  same_context(ctx, S);
+  same_context(ctx, T);
+  same_context(ctx, D);
+  if (!type_is_float((int)D.desc.Type))
+    fail(CL_INVALID_VALUE, "non-float image used when not allowed");
+  if (S.desc.Channels != T.desc.Channels || S.desc.Channels != D.desc.Channels)
+    fail(CL_INVALID_VALUE, "Different number of channels used");
+  if (S.desc.Width != D.desc.Width || S.desc.Height != D.desc.Height)
+    fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  if (T.desc.Width > S.desc.Width || T.desc.Height > S.desc.Height)
+    fail(CL_IMAGE_FORMAT_NOT_SUPPORTED, "The template image must be smaller than source image.");
+  if (!same_type(S, T))
+    fail(CL_IMAGE_FORMAT_MISMATCH, "The source image and the template image must be same type.");
+  proximity_run(ctx, m, S, T, D, OCIP_PATH_TENSOR);
+}
+
+Program& program(ocipProgram h, int kind) {
+  Program* p = reinterpret_cast<Program*>(h);
+  if (p == nullptr || p->magic != Program::kMagic || p->kind != kind)
+    fail(CL_INVALID_PROGRAM, "invalid program handle");
+  return *p;
+}
+
+void integral_prepare(Program& prog, const Image& src) {
+  const size_t need = integral_scratch_bytes((int)src.desc.Width, (int)src.desc.Height,
+                                             (int)src.desc.Channels);
+  if (prog.scratch_bytes >= need) return;
+  if (prog.scratch) {
+    check_cuda(cudaStreamSynchronize(prog.ctx->stream), "integral scratch sync");
+    cudaFree(prog.scratch);
+    prog.scratch = nullptr;
+    prog.scratch_bytes = 0;
+  }
+  check_cuda(cudaMalloc(&prog.scratch, need), "integral scratch allocation");
+  prog.scratch_bytes = need;
+}
+
+void integral(bool sqr, ocipProgram hp, ocipImage hs, ocipImage hd) {
+  Context& ctx = current();
+  Program& prog = program(hp, Program::kIntegral);
+  Image& S = image(hs);
+  Image& D = image(hd);
+  same_context(ctx, S);
+  same_context(ctx, D);
+  if (prog.ctx != &ctx) fail(CL_INVALID_CONTEXT, "program belongs to another context");
+  if (D.desc.Type != SImage::F32 && D.desc.Type != SImage::F64)
+    fail(CL_INVALID_VALUE, "Destination image of Integral must be F32 or F64");
+  integral_prepare(prog, S);
+  if (S.desc.Width != D.desc.Width || S.desc.Height != D.desc.Height)
+    fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  if (S.desc.Channels != D.desc.Channels)
+    fail(CL_INVALID_VALUE, "Different number of channels used");
+  send_if_needed(S);
+  check_cuda(launch_integral(sqr, dev_view(S), dev_view(D), prog.scratch, prog.scratch_bytes,
+                             ctx.stream),
+             "integral kernel launch");
+  D.in_device = true;
+}
+
+}  // namespace
+}  // namespace ocipb
+
+extern "C" {
+
+ocipError ocipPrepareProximity(ocipImage Image) {
+  OCIP_GUARD(
+    current();
+    if (Image != nullptr) image(Image);
+  )
+}
+
+ocipError ocipSqrDistance_Norm(ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity(kSqrDistanceNorm, S, T, D))
+}
+ocipError ocipSqrDistance(ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity(kSqrDistance, S, T, D))
+}
+ocipError ocipAbsDistance(ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity(kAbsDistance, S, T, D))
+}
+ocipError ocipCrossCorr(ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity(kCrossCorr, S, T, D))
+}
+ocipError ocipCrossCorr_Norm(ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity(kCrossCorrNorm, S, T, D))
+}
+
+ocipError ocipPrepareIntegral(ocipProgram* ProgramPtr, ocipImage Img) {
+  OCIP_GUARD(
+    Context& ctx = current();
+    if (ProgramPtr == nullptr) fail(CL_INVALID_VALUE, "ProgramPtr is NULL");
+    Program* p = new Program();
+    p->kind = Program::kIntegral;
+    p->ctx = &ctx;
+    *ProgramPtr = reinterpret_cast<ocipProgram>(p);
+    if (Img != nullptr) integral_prepare(*p, image(Img));
+  )
+}
+
+ocipBool ocipIsFFTAvailable(void) { return 1; }
+
+ocipError ocipPrepareImageProximityFFT(ocipProgram* ProgramPtr, ocipImage Img, ocipImage Tmpl) {
+  OCIP_GUARD(
+    Context& ctx = current();
+    if (ProgramPtr == nullptr) fail(CL_INVALID_VALUE, "ProgramPtr is NULL");
+    if (Img != nullptr) image(Img);
+    if (Tmpl != nullptr) image(Tmpl);
+    Program* p = new Program();
+    p->kind = Program::kProximityFFT;
+    p->ctx = &ctx;
+    *ProgramPtr = reinterpret_cast<ocipProgram>(p);
+  )
+}
+ocipError ocipSqrDistanceFFT(ocipProgram P, ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity_fft(kSqrDistance, P, S, T, D))
+}
+ocipError ocipSqrDistanceFFT_Norm(ocipProgram P, ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity_fft(kSqrDistanceNorm, P, S, T, D))
+}
+ocipError ocipCrossCorrFFT(ocipProgram P, ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity_fft(kCrossCorr, P, S, T, D))
+}
+ocipError ocipCrossCorrFFT_Norm(ocipProgram P, ocipImage S, ocipImage T, ocipImage D) {
+  OCIP_GUARD(proximity_fft(kCrossCorrNorm, P, S, T, D))
+}
+
+ocipError ocipIntegral(ocipProgram P, ocipImage S, ocipImage D) { OCIP_GUARD(integral(false, P, S, D)) }
+ocipError ocipSqrIntegral(ocipProgram P, ocipImage S, ocipImage D) { OCIP_GUARD(integral(true, P, S, D)) }
+
+}  // extern "C"

@@ -27,11 +27,13 @@
 extern "C" {
 #endif
 
-/* Reference arithmetic; dst holds REAL (float, or double for F64 sources). */
+/* Reference arithmetic; dst holds REAL (float, or double for F64 sources).
+ * fused = 0: every operation rounded separately; fused = 1: each
+ * `acc += a * b` of the reference evaluated as fma(a, b, acc). */
 int orc_proximity_refexact(int measure, int type, int nch, const void* src,
                            int src_step, const void* tmpl, int tmpl_step,
                            void* dst, int dst_step, int W, int H, int tw, int th,
-                           int row_begin, int row_end);
+                           int row_begin, int row_end, int fused);
 
 /* Exact / extended precision; dst is double[H][W*nch] (dense). */
 int orc_proximity_exact(int measure, int type, int nch, const void* src,

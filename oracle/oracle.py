@@ -81,14 +81,29 @@ def real_dtype(src):
     return np.float64 if src.dtype == np.float64 else np.float32
 
 
-def proximity_reference(measure, src, tmpl, mode=0, rows=None):
+_ref_fma = None
+
+
+def _lib_ref_fma():
+    global _ref_fma
+    if _ref_fma is None:
+        path = os.path.join(HERE, "_ref", "libocl_ref_fma.so")
+        if not os.path.exists(path):
+            raise RuntimeError("reference kernels not built: run `make -C oracle ref`")
+        _ref_fma = ctypes.CDLL(path)
+    return _ref_fma
+
+
+def proximity_reference(measure, src, tmpl, mode=0, rows=None, fused=False):
     """Run the reference's own kernel source (through the shim).
 
     mode 0 = the reference host's choice (_Cached iff template <= 16x16),
     1 = plain kernel, 2 = _Cached kernel. rows = (begin, end) limits the
-    computed band (other rows of the result stay 0).
+    computed band (other rows of the result stay 0). fused selects the build
+    with FP contraction (every acc += a*b as one fma), as GPU OpenCL
+    compilers build the kernels.
     """
-    lib = _lib_ref()
+    lib = _lib_ref_fma() if fused else _lib_ref()
     src, sp, ss, w, h, c = _img(src)
     tmpl, tp, ts, tw, th, tc = _img(tmpl)
     assert tc == c and tmpl.dtype == src.dtype
@@ -117,8 +132,9 @@ def integral_reference(src, sqr, dst_f64):
     return out
 
 
-def proximity_refexact(measure, src, tmpl, rows=None):
-    """This repository's restatement of the reference arithmetic (REAL)."""
+def proximity_refexact(measure, src, tmpl, rows=None, fused=False):
+    """This repository's restatement of the reference arithmetic (REAL);
+    fused=True evaluates each acc += a*b as fma(a, b, acc)."""
     lib = _lib_orc()
     src, sp, ss, w, h, c = _img(src)
     tmpl, tp, ts, tw, th, tc = _img(tmpl)
@@ -128,7 +144,8 @@ def proximity_refexact(measure, src, tmpl, rows=None):
     rc = lib.orc_proximity_refexact(measure_index(measure), type_index(src), c,
                                     sp, ss, tp, ts,
                                     out.ctypes.data_as(ctypes.c_void_p),
-                                    out.strides[0], w, h, tw, th, r0, r1)
+                                    out.strides[0], w, h, tw, th, r0, r1,
+                                    int(bool(fused)))
     if rc:
         raise RuntimeError(f"oracle returned {rc}")
     return out

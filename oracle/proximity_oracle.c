@@ -9,6 +9,11 @@
  *   - pixels outside the source read as 0 (ImageProximity.cl:64-67);
  *   - the _Norm measures divide by sqrt(sum S^2 * sum T^2) over the window,
  *     raw energies without mean removal (ImageProximity.cl:155, :409).
+ * The reference arithmetic comes in two forms: each operation rounded on its
+ * own (an OpenCL compiler that does not contract), or every `acc += a * b`
+ * contracted to fma(a, b, acc) (what GPU OpenCL compilers do by default;
+ * OpenCL C allows it). Both forms are pinned against the reference kernel
+ * source built without and with FP contraction.
  */
 #include <math.h>
 #include <stdint.h>
@@ -83,7 +88,7 @@ static int check_args(int measure, int type, int nch, int W, int H, int tw,
  * operation. */
 static void ref_f32(int measure, int type, int nch, const void* src, int ss,
                     const void* tmpl, int ts, void* dst, int ds, int W, int H,
-                    int tw, int th, int r0, int r1) {
+                    int tw, int th, int r0, int r1, int fused) {
   const int left = -tw / 2, top = -th / 2;
 #pragma omp parallel for schedule(dynamic, 4)
   for (int gy = r0; gy < r1; ++gy) {
@@ -98,6 +103,25 @@ static void ref_f32(int measure, int type, int nch, const void* src, int ss,
             float s = 0.f;
             if (!(px < 0 || py < 0 || px >= W || py >= H))
               s = load_f(pix(src, ss, type, nch, px, py, c), type);
+            if (fused) {
+              const float d = s - t;
+              switch (measure) {
+                case 0: sum = fmaf(d, d, sum); break;
+                case 1:
+                  sum = fmaf(d, d, sum);
+                  sumSS = fmaf(s, s, sumSS);
+                  sumTT = fmaf(t, t, sumTT);
+                  break;
+                case 2: sum += fabsf(d); break;
+                case 3: sum = fmaf(s, t, sum); break;
+                default:
+                  sum = fmaf(s, t, sum);
+                  sumSS = fmaf(s, s, sumSS);
+                  sumTT = fmaf(t, t, sumTT);
+                  break;
+              }
+              continue;
+            }
             switch (measure) {
               case 0: sum += (s - t) * (s - t); break;
               case 1:
@@ -125,7 +149,7 @@ static void ref_f32(int measure, int type, int nch, const void* src, int ss,
 /* Double precision body: REAL = double (F64 sources, Buffers.h:57-64). */
 static void ref_f64(int measure, int nch, const void* src, int ss,
                     const void* tmpl, int ts, void* dst, int ds, int W, int H,
-                    int tw, int th, int r0, int r1) {
+                    int tw, int th, int r0, int r1, int fused) {
   const int left = -tw / 2, top = -th / 2;
 #pragma omp parallel for schedule(dynamic, 4)
   for (int gy = r0; gy < r1; ++gy) {
@@ -140,6 +164,25 @@ static void ref_f64(int measure, int nch, const void* src, int ss,
             double s = 0.;
             if (!(px < 0 || py < 0 || px >= W || py >= H))
               s = load_d(pix(src, ss, 7, nch, px, py, c), 7);
+            if (fused) {
+              const double d = s - t;
+              switch (measure) {
+                case 0: sum = fma(d, d, sum); break;
+                case 1:
+                  sum = fma(d, d, sum);
+                  sumSS = fma(s, s, sumSS);
+                  sumTT = fma(t, t, sumTT);
+                  break;
+                case 2: sum += fabs(d); break;
+                case 3: sum = fma(s, t, sum); break;
+                default:
+                  sum = fma(s, t, sum);
+                  sumSS = fma(s, s, sumSS);
+                  sumTT = fma(t, t, sumTT);
+                  break;
+              }
+              continue;
+            }
             switch (measure) {
               case 0: sum += (s - t) * (s - t); break;
               case 1:
@@ -167,16 +210,16 @@ static void ref_f64(int measure, int nch, const void* src, int ss,
 int orc_proximity_refexact(int measure, int type, int nch, const void* src,
                            int src_step, const void* tmpl, int tmpl_step,
                            void* dst, int dst_step, int W, int H, int tw, int th,
-                           int row_begin, int row_end) {
+                           int row_begin, int row_end, int fused) {
   int e = check_args(measure, type, nch, W, H, tw, th);
   if (e) return e;
   if (row_end > H) row_end = H;
   if (type == 7)
     ref_f64(measure, nch, src, src_step, tmpl, tmpl_step, dst, dst_step, W, H,
-            tw, th, row_begin, row_end);
+            tw, th, row_begin, row_end, fused);
   else
     ref_f32(measure, type, nch, src, src_step, tmpl, tmpl_step, dst, dst_step,
-            W, H, tw, th, row_begin, row_end);
+            W, H, tw, th, row_begin, row_end, fused);
   return 0;
 }
 

@@ -46,6 +46,11 @@ static inline int get_local_size(int d) { return oclshim::g_lsize[d]; }
 static inline int get_group_id(int d) { return oclshim::g_grp[d]; }
 static inline void barrier(int) {}
 
+/* Single-precision overloads (the double ones come from <math.h>): a float
+ * argument must give a float result, as in OpenCL C. */
+static inline float fabs(float a) { return std::fabs(a); }
+static inline float sqrt(float a) { return std::sqrt(a); }
+
 /* OpenCL vector types: element-wise arithmetic, broadcast from a scalar,
  * .x/.y/.z/.w members and brace construction (`int2 Pos = {gx2, y};`). */
 template <class T, int N>
@@ -72,27 +77,70 @@ struct clvec : clvec_storage<T, N> {
   clvec(S v) {  // NOLINT: implicit broadcast, as `REAL sum = 0;` needs
     for (int i = 0; i < N; ++i) this->s[i] = T(v);
   }
+  template <class U>
+  clvec(const clvec<U, N>& o) {  // NOLINT: element-wise conversion
+    for (int i = 0; i < N; ++i) this->s[i] = T(o.s[i]);
+  }
   template <class A, class B, class... R>
   clvec(A a, B b, R... r) {
     const T v[N] = {T(a), T(b), T(r)...};
     for (int i = 0; i < N; ++i) this->s[i] = v[i];
   }
-#define CLVEC_OP(op)                                         \
-  friend clvec operator op(const clvec& a, const clvec& b) { \
-    clvec r;                                                 \
-    for (int i = 0; i < N; ++i) r.s[i] = a.s[i] op b.s[i];   \
-    return r;                                                \
-  }                                                          \
-  clvec& operator op##=(const clvec& b) {                    \
-    for (int i = 0; i < N; ++i) this->s[i] = this->s[i] op b.s[i]; \
-    return *this;                                            \
+  template <class U>
+  clvec& operator+=(const clvec<U, N>& b) {
+    for (int i = 0; i < N; ++i) this->s[i] += b.s[i];
+    return *this;
   }
-  CLVEC_OP(+)
-  CLVEC_OP(-)
-  CLVEC_OP(*)
-  CLVEC_OP(/)
-#undef CLVEC_OP
 };
+#define CLVEC_OP(op)                                                       \
+  template <class T, class U, int N>                                       \
+  static inline auto operator op(const clvec<T, N>& a, const clvec<U, N>& b) \
+      ->clvec<decltype(a.s[0] op b.s[0]), N> {                             \
+    clvec<decltype(a.s[0] op b.s[0]), N> r;                                \
+    for (int i = 0; i < N; ++i) r.s[i] = a.s[i] op b.s[i];                 \
+    return r;                                                              \
+  }
+CLVEC_OP(+)
+CLVEC_OP(-)
+CLVEC_OP(*)
+CLVEC_OP(/)
+#undef CLVEC_OP
+
+/* Contracted arithmetic (built with -DOCLSHIM_FUSED): `float` and `double`
+ * in the reference source become freal<F>, whose product is kept unrounded
+ * (fprod) until it is either added to an accumulator with `+=` -- one fused
+ * multiply-add, fma(a, b, acc), which is how an OpenCL compiler contracts
+ * `acc += a * b` -- or used in any other way, which rounds it first. */
+#ifdef OCLSHIM_FUSED
+template <class F>
+struct fprod {
+  F a, b;
+  operator F() const { return a * b; }
+};
+template <class F>
+struct freal {
+  F v;
+  freal() = default;
+  template <class S>
+  freal(S x) : v(F(x)) {}  // NOLINT
+  freal(fprod<F> p) : v(p.a * p.b) {}  // NOLINT
+  freal& operator+=(fprod<F> p) {
+    v = std::fma(p.a, p.b, v);
+    return *this;
+  }
+  freal& operator+=(freal o) {
+    v = v + o.v;
+    return *this;
+  }
+};
+template <class F> static inline fprod<F> operator*(freal<F> a, freal<F> b) { return {a.v, b.v}; }
+template <class F> static inline freal<F> operator-(freal<F> a, freal<F> b) { return freal<F>(a.v - b.v); }
+template <class F> static inline freal<F> operator+(freal<F> a, freal<F> b) { return freal<F>(a.v + b.v); }
+template <class F> static inline freal<F> operator/(freal<F> a, freal<F> b) { return freal<F>(a.v / b.v); }
+template <class F> static inline freal<F> fabs(freal<F> a) { return freal<F>(std::fabs(a.v)); }
+template <class F> static inline freal<F> sqrt(freal<F> a) { return freal<F>(std::sqrt(a.v)); }
+template <class F> static inline freal<F> sqrt(fprod<F> p) { return freal<F>(std::sqrt(p.a * p.b)); }
+#endif
 
 #define CLVEC_TYPES(base)              \
   typedef clvec<base, 2> base##2;      \
@@ -110,19 +158,15 @@ CLVEC_TYPES(double)
 template <class T, int N>
 static inline clvec<T, N> fabs(const clvec<T, N>& a) {
   clvec<T, N> r;
-  for (int i = 0; i < N; ++i) r.s[i] = std::fabs(a.s[i]);
+  for (int i = 0; i < N; ++i) r.s[i] = fabs(a.s[i]);
   return r;
 }
 template <class T, int N>
-static inline clvec<T, N> sqrt(const clvec<T, N>& a) {
-  clvec<T, N> r;
-  for (int i = 0; i < N; ++i) r.s[i] = std::sqrt(a.s[i]);
+static inline auto sqrt(const clvec<T, N>& a) -> clvec<decltype(sqrt(a.s[0])), N> {
+  clvec<decltype(sqrt(a.s[0])), N> r;
+  for (int i = 0; i < N; ++i) r.s[i] = sqrt(a.s[i]);
   return r;
 }
-/* Single-precision overloads (the double ones come from <math.h>): a float
- * argument must give a float result, as in OpenCL C. */
-static inline float fabs(float a) { return std::fabs(a); }
-static inline float sqrt(float a) { return std::sqrt(a); }
 
 /* convert_<REAL>(value): plain value conversion (round-to-nearest for the
  * integer-to-float case, which is exact for every type narrower than 24 bits). */
@@ -150,3 +194,24 @@ CLCONV_VEC(float, 4)
 CLCONV_VEC(double, 2)
 CLCONV_VEC(double, 4)
 #undef CLCONV_VEC
+
+#ifdef OCLSHIM_FUSED
+/* The reference source's `float` and `double` (through REAL, SCALAR and
+ * DOUBLE of cl-files/Buffers.h) name the contracted types from here on. The
+ * macros expand to single identifiers so that the source's token pasting
+ * (convert_##REAL, REAL##4) still forms valid names. */
+typedef freal<float> oclf32;
+typedef freal<double> oclf64;
+typedef clvec<oclf32, 2> oclf322;
+typedef clvec<oclf32, 4> oclf324;
+typedef clvec<oclf64, 2> oclf642;
+typedef clvec<oclf64, 4> oclf644;
+template <class S> static inline oclf32 convert_oclf32(S v) { return oclf32(v); }
+template <class S> static inline oclf64 convert_oclf64(S v) { return oclf64(v); }
+template <class S> static inline oclf322 convert_oclf322(const clvec<S, 2>& v) { return oclf322(v); }
+template <class S> static inline oclf324 convert_oclf324(const clvec<S, 4>& v) { return oclf324(v); }
+template <class S> static inline oclf642 convert_oclf642(const clvec<S, 2>& v) { return oclf642(v); }
+template <class S> static inline oclf644 convert_oclf644(const clvec<S, 4>& v) { return oclf644(v); }
+#define float oclf32
+#define double oclf64
+#endif
