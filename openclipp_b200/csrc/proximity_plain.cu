@@ -257,20 +257,29 @@ __global__ void __launch_bounds__(kThreads, 1)
 // recomputes it inside every output's loop (ImageProximity.cl:152, :406),
 // always with the same operands in the same order.
 template <int TYPE, typename CT>
-__global__ void template_energy_kernel(const char* tmpl, size_t pitch, int nch,
-                                       int tw, int th, CT* out) {
+__global__ void __launch_bounds__(256) template_energy_kernel(const char* tmpl, size_t pitch,
+                                                              int nch, int tw, int th, CT* out) {
   using ET = typename ElemOf<TYPE>::T;
+  constexpr int kMaxStage = 32768 / (int)sizeof(CT);
+  __shared__ CT st[kMaxStage];
   const int c = blockIdx.x;
-  if (threadIdx.x != 0) return;
   CT s = CT(0);
-  for (int h = 0; h < th; ++h) {
-    const ET* row = reinterpret_cast<const ET*>(tmpl + (size_t)h * pitch);
-    for (int w = 0; w < tw; ++w) {
-      const CT t = (CT)row[(size_t)w * nch + c];
-      s = mad(t, t, s);
+  // The template is staged in shared memory in chunks (all threads load), then
+  // one thread runs the chain: the order of the additions is the reference's.
+  for (int base = 0; base < th * tw; base += kMaxStage) {
+    const int n = min(kMaxStage, th * tw - base);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int h = (base + i) / tw, w = (base + i) - h * tw;
+      st[i] = (CT)reinterpret_cast<const ET*>(tmpl + (size_t)h * pitch)[(size_t)w * nch + c];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll 8
+      for (int i = 0; i < n; ++i) s = mad(st[i], st[i], s);
     }
   }
-  out[c] = s;
+  if (threadIdx.x == 0) out[c] = s;
 }
 
 template <int TYPE, typename CT, int MEAS>
@@ -312,7 +321,7 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
 
   constexpr bool kNorm = (MEAS == kCrossCorrNorm || MEAS == kSqrDistanceNorm);
   if (kNorm) {
-    template_energy_kernel<TYPE, CT><<<src.nch, 32, 0, st>>>(
+    template_energy_kernel<TYPE, CT><<<src.nch, 256, 0, st>>>(
         (const char*)tmpl.ptr, tmpl.pitch, tmpl.nch, p.tw, p.th, (CT*)tt_buf);
     count_launches(1);
   }

@@ -1,0 +1,155 @@
+"""Tensor-core (tcgen05) ImageProximity path, through the C ABI.
+
+Bars:
+  * U8 sources (i8 MMA, exact s32 sums, exact window statistics): results are
+    bit-identical to the plain path, which equals the reference wherever the
+    reference's float sums are exact;
+  * F32 sources (split BF16 hi/lo, three MMAs, FP64 window statistics):
+    relative error <= 1e-5 against the long-double oracle for CrossCorr and
+    the _Norm measures; SqrDistance (which cancels to 0 at a match) within
+    1e-5 of the scale sum S^2 + sum T^2 of its window.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MEAS = ["SqrDistance", "SqrDistance_Norm", "AbsDistance", "CrossCorr", "CrossCorr_Norm"]
+TOL = 1e-5
+
+
+def run(ocip, ctx, m, S, T, path, out_dtype=None):
+    ctx.set_path(path)
+    got = ocip.match(MEAS[m], S, T, out_dtype)
+    return got, ctx.last_path()
+
+
+def f32_check(got, S, T, m):
+    ex = O.proximity_exact(m, S, T)
+    if m == 0:
+        ss, _, tt = O.window_terms_exact(S, T)
+        scale = ss + tt[0]
+        err = np.abs(got - ex) / np.maximum(scale, 1e-30)
+    else:
+        fin = np.isfinite(ex)
+        assert np.array_equal(np.isfinite(got), fin)
+        err = np.abs(got[fin] - ex[fin]) / np.maximum(np.abs(ex[fin]), 1e-30)
+    assert err.max() <= TOL, f"{MEAS[m]}: max rel err {err.max():.3g}"
+    return float(err.max())
+
+
+@pytest.mark.parametrize("th,tw", [(31, 31), (16, 16), (1, 1), (3, 7), (17, 40), (32, 32),
+                                   (64, 64), (64, 5), (9, 64)])
+def test_u8_tensor_equals_plain(ocip, ctx, th, tw):
+    ctx.make_current()
+    rng = np.random.default_rng(th * 100 + tw)
+    S = rng.integers(0, 256, (150, 301), dtype=np.uint8)
+    T = rng.integers(0, 256, (th, tw), dtype=np.uint8)
+    for m in (0, 1, 3, 4):
+        plain, p1 = run(ocip, ctx, m, S, T, ocip.PATH_PLAIN)
+        tens, p2 = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert p1 == ocip.PATH_PLAIN and p2 == ocip.PATH_TENSOR
+        assert np.array_equal(plain, tens, equal_nan=True), MEAS[m]
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_u8_cfg1_exact_against_reference(ocip, ctx):
+    """512x512 U8, 16x16 template cut with noise: tensor path == reference."""
+    ctx.make_current()
+    rng = np.random.default_rng(1)
+    S = rng.integers(0, 256, (512, 512), dtype=np.uint8)
+    T = np.clip(S[100:116, 200:216].astype(np.int32) + np.round(rng.normal(0, 4, (16, 16))),
+                0, 255).astype(np.uint8)
+    for m in (0, 1, 3, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_AUTO)
+        assert path == ocip.PATH_TENSOR
+        ref = O.proximity_reference(m, S, T) if O.ref_available() else O.proximity_refexact(m, S, T)
+        assert np.array_equal(got, ref, equal_nan=True), MEAS[m]
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_u8_tall_image_many_bands(ocip, ctx):
+    """Enough rows for several bands per strip; exact integer results."""
+    ctx.make_current()
+    rng = np.random.default_rng(2)
+    S = rng.integers(0, 256, (2600, 140), dtype=np.uint8)
+    T = rng.integers(0, 256, (24, 24), dtype=np.uint8)
+    got, path = run(ocip, ctx, 3, S, T, ocip.PATH_TENSOR)
+    assert path == ocip.PATH_TENSOR
+    assert np.array_equal(got, O.proximity_exact(3, S, T).astype(np.float32))
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+@pytest.mark.parametrize("th,tw", [(31, 31), (16, 16), (1, 1), (5, 3), (17, 40), (32, 32),
+                                   (64, 64), (40, 9)])
+def test_f32_tensor_accuracy(ocip, ctx, th, tw):
+    ctx.make_current()
+    rng = np.random.default_rng(th * 7 + tw)
+    S = rng.random((130, 263)).astype(np.float32)
+    T = rng.random((th, tw)).astype(np.float32)
+    for m in (0, 1, 3, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert path == ocip.PATH_TENSOR
+        f32_check(got, S, T, m)
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_f32_blob_field_crop_accuracy(ocip, ctx):
+    """The benchmark's data (blob field + noise, template cut from it) on a
+    crop: max relative error per measure."""
+    import bench
+    ctx.make_current()
+    S = bench.blob_field(600, 500, nblobs=20, seed=3)
+    T = S[200:231, 300:331].copy()
+    for m in (0, 1, 3, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert path == ocip.PATH_TENSOR
+        f32_check(got, S, T, m)
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_f32_signed_values(ocip, ctx):
+    ctx.make_current()
+    rng = np.random.default_rng(4)
+    S = rng.standard_normal((97, 200)).astype(np.float32)
+    T = rng.standard_normal((12, 13)).astype(np.float32)
+    got, _ = run(ocip, ctx, 3, S, T, ocip.PATH_TENSOR)
+    ex = O.proximity_exact(3, S, T)
+    # with signed data the sum can cancel: compare against the sum of |S*T|
+    absref = O.proximity_exact(3, np.abs(S), np.abs(T))
+    assert (np.abs(got - ex) / absref).max() <= TOL
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_fallbacks_to_plain(ocip, ctx):
+    """AbsDistance, multi-channel and large templates are served by the plain
+    path even when the tensor path is requested."""
+    ctx.make_current()
+    rng = np.random.default_rng(5)
+    S = rng.random((80, 90)).astype(np.float32)
+    T = rng.random((7, 7)).astype(np.float32)
+    _, path = run(ocip, ctx, 2, S, T, ocip.PATH_TENSOR)
+    assert path == ocip.PATH_PLAIN
+    S4 = rng.random((40, 50, 4)).astype(np.float32)
+    _, path = run(ocip, ctx, 3, S4, rng.random((5, 5, 4)).astype(np.float32), ocip.PATH_TENSOR)
+    assert path == ocip.PATH_PLAIN
+    _, path = run(ocip, ctx, 3, rng.random((100, 100)).astype(np.float32),
+                  rng.random((65, 65)).astype(np.float32), ocip.PATH_TENSOR)
+    assert path == ocip.PATH_PLAIN
+    # AUTO keeps F32 on the plain path (not bit-exact on the tensor path)
+    _, path = run(ocip, ctx, 3, S, T, ocip.PATH_AUTO)
+    assert path == ocip.PATH_PLAIN
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_f64_destination(ocip, ctx):
+    ctx.make_current()
+    rng = np.random.default_rng(6)
+    S = rng.integers(0, 256, (64, 140), dtype=np.uint8)
+    T = rng.integers(0, 256, (8, 8), dtype=np.uint8)
+    got, path = run(ocip, ctx, 0, S, T, ocip.PATH_TENSOR, out_dtype=np.float64)
+    assert path == ocip.PATH_TENSOR
+    assert np.array_equal(got, O.proximity_exact(0, S, T))
+    ctx.set_path(ocip.PATH_PLAIN)
