@@ -128,7 +128,7 @@ __device__ __forceinline__ void apply_chunk(CT (&acc)[RX], CT (&acc2)[RX],
 }
 
 template <int TYPE, typename CT, int MEAS, int RY>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     prox_plain_kernel(const PlainParams p) {
   using ET = typename ElemOf<TYPE>::T;
   constexpr bool kNorm = (MEAS == kCrossCorrNorm || MEAS == kSqrDistanceNorm);
@@ -222,9 +222,23 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (h < 0 || h >= p.th) continue;
           const CT* trow = s_t + (size_t)(h - tg0) * p.twp + wc * WCH;
           CT tv[WCH];
+          if (sizeof(CT) == 4) {
+            const float4 a = reinterpret_cast<const float4*>(trow)[0];
+            const float4 b = reinterpret_cast<const float4*>(trow)[1];
+            tv[0] = (CT)a.x; tv[1] = (CT)a.y; tv[2] = (CT)a.z; tv[3] = (CT)a.w;
+            tv[4] = (CT)b.x; tv[5] = (CT)b.y; tv[6] = (CT)b.z; tv[7] = (CT)b.w;
+          } else {
 #pragma unroll
-          for (int k = 0; k < WCH; ++k) tv[k] = trow[k];
-          apply_chunk<CT, MEAS>(acc[j], acc2[j], win, tv, kmax);
+            for (int k = 0; k < WCH / 2; ++k) {
+              const double2 d = reinterpret_cast<const double2*>(trow)[k];
+              tv[2 * k] = (CT)d.x;
+              tv[2 * k + 1] = (CT)d.y;
+            }
+          }
+          if (kmax == WCH)
+            apply_chunk<CT, MEAS>(acc[j], acc2[j], win, tv, WCH);
+          else
+            apply_chunk<CT, MEAS>(acc[j], acc2[j], win, tv, kmax);
         }
       }
     }

@@ -622,7 +622,10 @@ bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl, const
   if (src.nch != 1 || tmpl.nch != 1 || dst.nch != 1) return false;
   if (tmpl.width > 64 || tmpl.height > 64) return false;
   if (src.type == U8) return true;
-  if (src.type == F32) return forced;
+  // F32: the BF16 hi + lo split keeps about 16 bits of each operand, so one
+  // product can be off by ~3e-5 relative; the <= 1e-5 bar needs the errors of
+  // many terms to average, and tiny templates gain nothing from the MMA.
+  if (src.type == F32) return forced && tmpl.width * tmpl.height >= 64;
   return false;
 }
 

@@ -82,8 +82,8 @@ def test_u8_tall_image_many_bands(ocip, ctx):
     ctx.set_path(ocip.PATH_PLAIN)
 
 
-@pytest.mark.parametrize("th,tw", [(31, 31), (16, 16), (1, 1), (5, 3), (17, 40), (32, 32),
-                                   (64, 64), (40, 9)])
+@pytest.mark.parametrize("th,tw", [(31, 31), (16, 16), (8, 8), (17, 40), (32, 32),
+                                   (64, 64), (40, 9), (2, 64)])
 def test_f32_tensor_accuracy(ocip, ctx, th, tw):
     ctx.make_current()
     rng = np.random.default_rng(th * 7 + tw)
@@ -140,6 +140,9 @@ def test_fallbacks_to_plain(ocip, ctx):
     assert path == ocip.PATH_PLAIN
     # AUTO keeps F32 on the plain path (not bit-exact on the tensor path)
     _, path = run(ocip, ctx, 3, S, T, ocip.PATH_AUTO)
+    assert path == ocip.PATH_PLAIN
+    # F32 templates under 64 taps stay on the plain path
+    _, path = run(ocip, ctx, 3, S, rng.random((5, 3)).astype(np.float32), ocip.PATH_TENSOR)
     assert path == ocip.PATH_PLAIN
     ctx.set_path(ocip.PATH_PLAIN)
 
