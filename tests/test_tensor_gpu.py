@@ -6,8 +6,9 @@ Bars:
     reference's float sums are exact;
   * F32 sources (split BF16 hi/lo, three MMAs, FP64 window statistics):
     relative error <= 1e-5 against the long-double oracle for CrossCorr and
-    the _Norm measures; SqrDistance (which cancels to 0 at a match) within
-    1e-5 of the scale sum S^2 + sum T^2 of its window.
+    CrossCorr_Norm; SqrDistance[_Norm] (which cancel to 0 at a match) within
+    1e-5 of the scale of their terms, sum S^2 + sum T^2 of the window
+    (divided by sqrt(sum S^2 * sum T^2) for the _Norm form).
 """
 import numpy as np
 import pytest
@@ -28,10 +29,15 @@ def run(ocip, ctx, m, S, T, path, out_dtype=None):
 
 def f32_check(got, S, T, m):
     ex = O.proximity_exact(m, S, T)
-    if m == 0:
+    if m in (0, 1):
+        # SqrDistance[_Norm] cancel to 0 at a match: error relative to the
+        # scale of the terms, (sum S^2 + sum T^2) [/ sqrt(sum S^2 * sum T^2)].
         ss, _, tt = O.window_terms_exact(S, T)
         scale = ss + tt[0]
-        err = np.abs(got - ex) / np.maximum(scale, 1e-30)
+        if m == 1:
+            scale = scale / np.sqrt(ss * tt[0])
+        fin = np.isfinite(scale)
+        err = np.abs(got[fin] - ex[fin]) / np.maximum(scale[fin], 1e-30)
     else:
         fin = np.isfinite(ex)
         assert np.array_equal(np.isfinite(got), fin)
