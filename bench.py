@@ -164,6 +164,7 @@ def run_ours(args, world, rank, local):
 
     S, T = workload(seed=1234 + rank)
     H, W = S.shape
+    MEASURES = args.measures
     taps_step = valid_taps(W, H, T_SIDE, T_SIDE) * len(MEASURES)
 
     ctx = ocip.Context(local)
@@ -227,14 +228,14 @@ def run_ours(args, world, rank, local):
     clocks = clk.summary()
 
     # Accuracy of this run's maps against an FP64 oracle on a crop.
-    errs = accuracy_report(S, T, outs, Ds) if rank == 0 else {}
+    errs = accuracy_report(S, T, outs, Ds, MEASURES) if rank == 0 else {}
 
-    # End-to-end arm: pinned host buffers, send + 5 calls + 5 reads per step.
-    e2e_ms = run_e2e(args, ocip, torch, ctx, S, T, stream)
+    # End-to-end arm: pinned host buffers, send + calls + reads per step.
+    e2e_ms = run_e2e(args, ocip, torch, ctx, S, T, stream) if not args.no_e2e else float("nan")
     e2e_ms = allreduce_max(e2e_ms)
 
     value = taps_step * world / (ms_step * 1e-3) / 1e9
-    e2e_value = taps_step * world / (e2e_ms * 1e-3) / 1e9
+    e2e_value = taps_step * world / (e2e_ms * 1e-3) / 1e9 if e2e_ms == e2e_ms else None
 
     # Roofline of the dominant kernel (largest share of the step).
     med = {m: float(np.median(v)) for m, v in per_kernel.items()}
@@ -263,7 +264,7 @@ def run_ours(args, world, rank, local):
         "per_measure_gtaps": {m: round(taps_meas / (v * 1e-3) / 1e9, 1) for m, v in med.items()},
         "accuracy_vs_fp64": errs,
         "roofline": roof,
-        "e2e": {"value": round(e2e_value, 2), "unit": "Gtaps/s",
+        "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Gtaps/s",
                 "h2d_bytes_per_step": int(S.nbytes + T.nbytes),
                 "d2h_bytes_per_step": int(sum(o.nbytes for o in outs))},
         "gpu_launches": int(launches),
@@ -280,6 +281,7 @@ def run_ours(args, world, rank, local):
 
 
 def run_e2e(args, ocip, torch, ctx, S, T, stream):
+    MEASURES = args.measures
     H, W = S.shape
     hS = torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy()
     hS[:] = S
@@ -314,7 +316,7 @@ def run_e2e(args, ocip, torch, ctx, S, T, stream):
     return float(np.mean(times))
 
 
-def accuracy_report(S, T, outs, Ds):
+def accuracy_report(S, T, outs, Ds, measures):
     """Max abs / relative error of each map vs the FP64 oracle on a crop."""
     from oracle import oracle as O
     for D in Ds:
@@ -322,8 +324,8 @@ def accuracy_report(S, T, outs, Ds):
     y0, x0, n = 1000, 1000, 192
     crop = S[y0 - 20:y0 + n + 20, x0 - 20:x0 + n + 20]
     rep = {}
-    for i, m in enumerate(MEASURES):
-        ex = O.proximity_exact(i, crop, T)[20:-20, 20:-20]
+    for i, m in enumerate(measures):
+        ex = O.proximity_exact(MEASURES.index(m), crop, T)[20:-20, 20:-20]
         got = outs[i][y0:y0 + n, x0:x0 + n].astype(np.float64)
         scale = np.abs(ex).max()
         rel = np.abs(got - ex) / np.maximum(np.abs(ex), 1e-300)
@@ -411,7 +413,12 @@ def main():
     ap.add_argument("--path", choices=["auto", "tensor", "plain"], default="tensor")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--measures", default=",".join(MEASURES),
+                    help="comma-separated subset of the five measures (profiling)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm (profiling)")
     args = ap.parse_args()
+    args.measures = [m for m in args.measures.split(",") if m]
+    assert all(m in MEASURES for m in args.measures), args.measures
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
