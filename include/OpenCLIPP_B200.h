@@ -44,6 +44,26 @@ ocipError ocip_API ocipGetStream(void** Stream);
 /* Number of CUDA kernels this library has launched in this process. */
 ocipError ocip_API ocipGetLaunchCount(uint64_t* Count);
 
+/* Integral (Square = 0) or SqrIntegral (Square != 0) that allocates no device
+ * memory. It has no counterpart in the reference.
+ * It is for callers that cannot let a library call cudaMalloc: their device
+ * memory belongs to another allocator, or they must not allocate while running
+ * because allocation can block and synchronise the device. The caller passes
+ * device pointers and row pitches (bytes) for Source and Dest, their SImage
+ * descriptions (Step is ignored; the pitches are used) and a cudaStream_t
+ * (NULL for the default stream); the work is queued on that stream on the
+ * calling thread's current CUDA device, and no context is needed.
+ * The scan's scratch is a fixed 8 MiB array that every device which loads
+ * the library holds until the process exits; images whose scratch would not
+ * fit (about 6000 x 6000 pixels per channel) are refused with
+ * CL_INVALID_IMAGE_SIZE. The first call on a device looks up that array's
+ * device address; make that first call before capturing the stream into a
+ * CUDA graph. All calls share the array: calls that overlap on the GPU (on
+ * different streams, or on the same device from several threads) race. */
+ocipError ocip_API ocipIntegralNoAlloc(int Square, SImage SourceDesc, const void* Source,
+                                       size_t SourcePitch, SImage DestDesc, void* Dest,
+                                       size_t DestPitch, void* Stream);
+
 /* Device address and row pitch (bytes) of an image's device buffer. */
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,
                                          size_t* Pitch);

@@ -279,3 +279,98 @@ cudaError_t launch_integral(bool sqr, const DevImage& src, const DevImage& dst,
 }
 
 }  // namespace ocipb
+
+// ---- Integral without device allocation -------------------------------------
+//
+// Some callers cannot let a library allocate device memory: their device
+// memory is owned by another allocator (a framework's memory pool that holds
+// the whole budget), or they must not allocate once running, because
+// cudaMalloc/cudaFree can block and synchronise the whole device (for example
+// latency-bound video pipelines). ocipIntegralNoAlloc serves them: the scan's
+// scratch lives in the fixed array below, reserved when the library is loaded
+// on a device and held by every device that loads the library until the
+// process exits.
+
+namespace ocipb {
+namespace {
+
+// Largest scratch the allocation-free entry point can use: 8 MiB, enough for
+// one channel up to about 6000 x 6000 pixels (integral_scratch_bytes()).
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on the current device. Host code
+// cannot use the array's name as a device address; cudaGetSymbolAddress gives
+// the real one, once per device (on the first call made on that device).
+cudaError_t noalloc_scratch(int dev, void** ptr) {
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *ptr = g_noalloc_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace ocipb
+
+#include <string>
+
+#include "../../include/OpenCLIPP.h"
+#include "../../include/OpenCLIPP_B200.h"
+#include "host.h"
+
+extern "C" ocipError ocipIntegralNoAlloc(int Square, SImage SourceDesc, const void* Source,
+                                         size_t SourcePitch, SImage DestDesc, void* Dest,
+                                         size_t DestPitch, void* Stream) {
+  using namespace ocipb;
+  OCIP_GUARD(
+    if (Source == nullptr || Dest == nullptr) fail(CL_INVALID_MEM_OBJECT, "NULL image pointer");
+    if ((int)SourceDesc.Type < 0 || (int)SourceDesc.Type >= (int)SImage::NbDataTypes ||
+        SourceDesc.Channels < 1 || SourceDesc.Channels > 4)
+      fail(CL_IMAGE_FORMAT_NOT_SUPPORTED, "unsupported source format");
+    if (DestDesc.Type != SImage::F32 && DestDesc.Type != SImage::F64)
+      fail(CL_INVALID_VALUE, "Destination image of Integral must be F32 or F64");
+    if (SourceDesc.Width != DestDesc.Width || SourceDesc.Height != DestDesc.Height)
+      fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+    if (SourceDesc.Channels != DestDesc.Channels)
+      fail(CL_INVALID_VALUE, "Different number of channels used");
+    if (SourceDesc.Width == 0 || SourceDesc.Height == 0)
+      fail(CL_INVALID_BUFFER_SIZE, "empty image");
+    if (SourcePitch < (size_t)SourceDesc.Width * SourceDesc.Channels * type_bytes((int)SourceDesc.Type) ||
+        DestPitch < (size_t)DestDesc.Width * DestDesc.Channels * type_bytes((int)DestDesc.Type))
+      fail(CL_INVALID_VALUE, "pitch smaller than one row of pixels");
+    const size_t need = integral_scratch_bytes((int)SourceDesc.Width, (int)SourceDesc.Height,
+                                               (int)SourceDesc.Channels);
+    if (need > kNoAllocScratchBytes)
+      fail(CL_INVALID_IMAGE_SIZE,
+           "image too large for ocipIntegralNoAlloc: needs " + std::to_string(need) +
+               " bytes of scratch, the fixed limit is " + std::to_string(kNoAllocScratchBytes));
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    void* scratch = nullptr;
+    check_cuda(noalloc_scratch(dev, &scratch), "cudaGetSymbolAddress");
+    DevImage s, d;
+    s.ptr = const_cast<void*>(Source);
+    s.pitch = SourcePitch;
+    s.width = (int)SourceDesc.Width;
+    s.height = (int)SourceDesc.Height;
+    s.nch = (int)SourceDesc.Channels;
+    s.type = (int)SourceDesc.Type;
+    d.ptr = Dest;
+    d.pitch = DestPitch;
+    d.width = (int)DestDesc.Width;
+    d.height = (int)DestDesc.Height;
+    d.nch = (int)DestDesc.Channels;
+    d.type = (int)DestDesc.Type;
+    check_cuda(launch_integral(Square != 0, s, d, scratch, kNoAllocScratchBytes,
+                               reinterpret_cast<cudaStream_t>(Stream)),
+               "integral kernel launch");
+  )
+}

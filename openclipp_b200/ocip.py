@@ -94,6 +94,8 @@ def _load():
         "ocipGetStream": (i32, [ctypes.POINTER(vp)]),
         "ocipGetImageDevicePtr": (i32, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t)]),
         "ocipGetLaunchCount": (i32, [ctypes.POINTER(ctypes.c_uint64)]),
+        "ocipIntegralNoAlloc": (i32, [ctypes.c_int, SImage, vp, ctypes.c_size_t, SImage, vp,
+                                      ctypes.c_size_t, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
