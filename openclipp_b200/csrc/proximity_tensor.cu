@@ -104,7 +104,9 @@ __host__ __device__ inline Layout make_layout(int elem, int R, int K, int nblk, 
   L.cum = L.pre + align128(2 * (boxw + 8) * 8);
   L.stg = L.cum + R * kM * 8;
   L.bars = L.stg + kG * kM * 16;
-  L.total = L.bars + 512;
+  // mbarriers (2 per raw, operand and TMEM stage, plus one), then the TMEM
+  // address, the abort flag and the template energy.
+  L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNQ + 2 * kSTM + 1) + 32);
   return L;
 }
 

@@ -45,6 +45,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait with a suspend-time hint (ns): the thread sleeps in hardware until
+// the phase completes or the hint expires, instead of spinning (spinning
+// waits flood the shared-memory pipe that the other roles need).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity,
+                                                    uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Waits for the phase with the given parity to complete. Gives up after
 // `limit` clock cycles or as soon as *abort is set, sets *abort and returns
 // false in that case, so that no thread of a kernel can wait forever.
@@ -52,14 +68,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile int* abort, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  for (uint32_t i = 0;; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 63) == 63) {
-      if (*abort) return false;
-      if (clock64() - t0 > limit) {
-        *abort = 1;
-        return false;
-      }
+  for (;;) {
+    if (mbar_try_wait_sleep(bar, parity, 200000u)) return true;
+    if (*abort) return false;
+    if (clock64() - t0 > limit) {
+      *abort = 1;
+      return false;
     }
   }
 }
