@@ -237,19 +237,34 @@ def run_ours(args, world, rank, local):
     value = taps_step * world / (ms_step * 1e-3) / 1e9
     e2e_value = taps_step * world / (e2e_ms * 1e-3) / 1e9 if e2e_ms == e2e_ms else None
 
-    # Roofline of the dominant kernel (largest share of the step).
+    # Roofline of the dominant tensor-core kernel (largest share of the step
+    # among the measures served by the tensor path); the plain kernels that
+    # remain in the step (AbsDistance has no product form) are reported beside
+    # it against the FP32 ALU rate.
     med = {m: float(np.median(v)) for m, v in per_kernel.items()}
-    dom = max(med, key=med.get)
+    tensor_meas = [m for m in med if paths_used[m] == "tensor"] or list(med)
+    dom = max(tensor_meas, key=med.get)
     peaks = load_peaks()
     taps_meas = valid_taps(W, H, T_SIDE, T_SIDE)
     same_taps = W * H * T_SIDE * T_SIDE
     tflops = 2.0 * same_taps / (med[dom] * 1e-3) / 1e12
     roof = {"kernel": f"{dom} ({paths_used[dom]})", "bound": "tensor", "achieved": round(tflops, 2),
             "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-            "frac": round(tflops / peaks["bf16_tflops"], 4), "traffic": None,
+            "frac": round(tflops / peaks["bf16_tflops"], 4),
+            "traffic": ncu_traffic(dom, paths_used[dom]),
             "peak_source": peaks["source"],
             "flops_convention": "2 per tap (one multiply-add), same-size map "
                                 f"{W}x{H}x{T_SIDE}x{T_SIDE} per launch"}
+    plain_meas = [m for m in med if paths_used[m] == "plain"]
+    roof_plain = {}
+    for m in plain_meas:
+        # FP32 lanes: 148 SMs x 128 lanes x 2 ops (sub, abs-add) per tap.
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        peak_taps = 148 * 128 * sm_mhz * 1e6 / 2.0
+        got = same_taps / (med[m] * 1e-3)
+        roof_plain[m] = {"bound": "alu (FP32 lanes)", "achieved_gtaps": round(got / 1e9, 1),
+                         "peak_gtaps": round(peak_taps / 1e9, 1), "frac": round(got / peak_taps, 4),
+                         "peak_source": "nominal: 148 SMs x 128 FP32 lanes x clock, 2 ops per tap"}
 
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "Gtaps/s", "n_gpus": world,
@@ -264,6 +279,7 @@ def run_ours(args, world, rank, local):
         "per_measure_gtaps": {m: round(taps_meas / (v * 1e-3) / 1e9, 1) for m, v in med.items()},
         "accuracy_vs_fp64": errs,
         "roofline": roof,
+        "roofline_plain": roof_plain,
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Gtaps/s",
                 "h2d_bytes_per_step": int(S.nbytes + T.nbytes),
                 "d2h_bytes_per_step": int(sum(o.nbytes for o in outs))},
@@ -332,6 +348,16 @@ def accuracy_report(S, T, outs, Ds, measures):
         rep[m] = {"max_abs": float(np.abs(got - ex).max()), "max_rel": float(rel.max()),
                   "max_abs_over_maxref": float(np.abs(got - ex).max() / scale)}
     return rep
+
+
+def ncu_traffic(measure, path):
+    """DRAM bytes (read + write) per launch of the given kernel from the
+    committed ncu summary, or None when that kernel was not captured."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(f"{measure} ({path})")
 
 
 def load_peaks():

@@ -220,6 +220,15 @@ ocipError ocipCreateImage(ocipImage* ImagePtr, SImage desc, void* ImageData,
       delete img;
       check_cuda(e, "image allocation");
     }
+    // Zero the whole buffer once: the bytes between a row's end and the next
+    // row (pitch padding) are never written afterwards, so kernels that read
+    // whole 16-byte chunks past the last pixel see zeros there.
+    e = cudaMemsetAsync(img->dev, 0, img->pitch * desc.Height, ctx.stream);
+    if (e != cudaSuccess) {
+      cudaFree(img->dev);
+      delete img;
+      check_cuda(e, "image initialisation");
+    }
     *ImagePtr = reinterpret_cast<ocipImage>(img);
   )
 }

@@ -3,43 +3,56 @@
 // The product term of SqrDistance[_Norm] and CrossCorr[_Norm]
 // (cl-files/ImageProximity.cl :44, :122, :290, :375),
 //   C(x, y) = sum_h sum_w S(x + w - tw/2, y + h - th/2) * T(w, h),
-// is computed as one small GEMM per source row r and 128-column strip:
-//   D_r[m][n] = sum_k A_r[m][k] * B[n][k],  A_r[m][k] = S(x0 + m + k - tw/2, r),
-//   B[n][k] = T(k, n - (R - th)) (template rows in N, zero rows on top),
-// M = 128 output positions, N = R (th rounded up to 16/32/64), K = tw rounded
-// up. Then C(x0 + m, y) = sum_n D_{y + n - off}[m][n], off = R - th + th/2:
-// every source row contributes to R output rows, one per template row. The
-// epilogue thread of lane m keeps those R partial sums in a register ring and
-// emits output row y as soon as its last template row has been added.
+// is computed as one small GEMM per source row r and 256-position strip.
+// Each TMEM lane m holds two output positions, x0 + 2m (phase 0) and
+// x0 + 2m + 1 (phase 1), and the A row of lane m is the source-row window
+//   A_r[m][k] = S(x0 - tw/2 + 2m + k, r),   k < K = roundup(tw + 1),
+// so the two phases share A: phase p reads it one pixel later. The template
+// operand has N = 2R rows (R = th rounded up to 16/32/64, zero rows on top),
+//   B[p R + n][k] = Tpad(k - p, n),   Tpad(w, n) = T(w, n - (R - th)),
+// and D_r[m][p R + n] is the contribution of template row n to position
+// x0 + 2m + p. Source row r feeds output row y = r - n + off
+// (off = R - th + th/2) through template row n, so every output row collects
+// R consecutive steps. The epilogue keeps those R partial sums per position
+// in registers, ordered by output row: at each step it adds the step's R
+// columns and shifts by one (acc[c] <- acc[c + 1] + D[R - 2 - c]), and
+// acc[0] + D[R - 1] is the finished output row.
 //
-// A_r is a Hankel (sliding-window) matrix. In the canonical K-major
-// SWIZZLE_NONE layout, core matrix (mb, kb) holds
-// S(x0 + 8(mb + kb) + row + j); it depends on mb + kb only. So A_r is given to
-// the tensor core as a descriptor with LBO = SBO = 128 bytes over an array of
-// 16 + K/8 - 1 core matrices, row q of which holds pixels q .. q+7: an 8x
-// expansion of the source row built in shared memory, instead of the 32x
-// (K-fold) expansion of an explicit im2col. For 8-bit sources (16 elements
-// per core-matrix row) the same holds with LBO = 256, SBO = 128.
+// The A operand lives in tensor memory: builder warps write each lane's
+// K-pixel window with tcgen05.st (BF16 hi/lo pairs for F32 sources, bytes
+// for U8), and the MMA reads it from TMEM, which costs half as many cycles
+// per instruction as an A operand read from shared memory.
 //
 // Precision. U8 sources use the i8 MMA with s32 accumulation: every product
 // term is exact and so are the results. F32 sources are split into BF16 hi + lo
 // parts (S = S_hi + S_lo + O(2^-18 S)); three MMAs (hi*hi, hi*lo, lo*hi)
-// accumulate in FP32 in TMEM. The window energy sum S^2 of each output comes
-// from FP64 running sums fused into the kernel (per row: a prefix sum over the
-// staged row gives the row-window sums; per column: a running sum over rows
-// and its value th rows earlier), the template energy is exact in FP64, and
-// SqrDistance = E_S - 2C + E_T and the _Norm divisions are done in FP64.
+// accumulate in FP32 in TMEM. The window energy sum S^2 of each position is
+// a per-row sum of tw squares (FP32 FMA for F32 sources, exact integers for
+// U8) and a running sum over the last th rows (FP64 / exact integers); the
+// template energy is exact in FP64. SqrDistance = E_S - 2C + E_T and the
+// _Norm divisions are done in FP64 (F32 sources) or as the plain path does
+// them (U8 sources).
 //
-// Roles (256 threads): warp 0 issues TMA loads of source rows (zero fill
-// outside the image), warp 1 allocates TMEM and issues the MMAs, warps 2-3
-// build the Hankel operands and row energies, warps 4-7 (TMEM lanes 0-127)
-// run the epilogue. Stages are chained by mbarriers; every wait is bounded
-// and sets an error flag instead of hanging.
+// Roles (17 warps; one CTA per SM, since it allocates all of TMEM):
+//   warps 0-7   builders, two per TMEM sub-partition (tcgen05.ld/st reach
+//               only the 32 lanes of the warp's sub-partition), one per phase:
+//               the A operand of step t (the warp's half of the K columns) and
+//               the window energy of its positions, handed to the epilogue
+//               through a shared-memory ring;
+//   warps 8-15  epilogue, same split: TMEM loads, running sums, output;
+//   warp 16     control: TMA loads of source rows (zero fill outside the
+//               image) and the MMAs of each step. Issuing an MMA or a commit
+//               blocks the issuing thread for tens of cycles, so this thread
+//               does nothing else: one wait (ready), the MMAs, one commit
+//               (mma_done) per step.
+// Stages are chained by mbarriers; every wait is bounded and sets an error
+// flag instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <type_traits>
 
@@ -51,24 +64,38 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kM = 128;
-constexpr int kThreads = 256;
-constexpr int kRawRows = 4;
-constexpr int kNRaw = 4;
-constexpr int kNQ = 8;
-constexpr int kSTM = 4;
-constexpr int kG = 8;  // epilogue output staging depth (steps)
+constexpr int kM = 128;                 // TMEM lanes = A rows
+constexpr int kPos = 2 * kM;            // output positions per strip
+constexpr int kBuilders = 8;
+constexpr int kEpilogue = 8;
+constexpr int kThreads = (kBuilders + kEpilogue + 1) * 32;  // + control warp
+constexpr int kRB = 8;                  // source rows per TMA load
+constexpr int kNRaw = 4;                // TMA stages
+constexpr int kNE = 16;                 // window-energy ring depth (steps)
+constexpr int kTmemCols = 512;
+constexpr int kMinSmem = 120 * 1024;    // keeps one CTA per SM (it takes all of TMEM)
 constexpr long long kSpinLimit = 4000000000LL;  // about 2 s of SM clock
 
 enum Elem { kF32 = 0, kU8 = 1 };
 
+// TMEM stages: NS stages of D (2R columns) first, then NS stages of A.
+template <int ELEM, int R, int K>
+struct Stages {
+  static constexpr int N2 = 2 * R;
+  static constexpr int AC = ELEM == kF32 ? K : K / 4;  // TMEM columns per A stage
+  static constexpr int NS0 = kTmemCols / (N2 + AC);
+  static constexpr int NS = NS0 > 4 ? 4 : NS0;
+  static_assert(NS >= 2, "TMEM too small for two stages");
+  static_assert(NS * (N2 + AC) <= kTmemCols, "TMEM too small for the stages");
+  static_assert(2 * NS <= kNE, "energy ring shorter than the pipeline");
+};
+
 struct TensorParams {
   int W, H;
   int tw, th;
-  int K;         // padded template width
-  int nblk;      // core-matrix blocks per Hankel array
-  int boxw;      // TMA box width (elements) = 128 + K
-  int xshift;    // strip b covers outputs [128 b - xshift, 128 b - xshift + 128)
+  int inner;     // elements per 16-byte group of the TMA view (4 F32, 16 U8)
+  int nbox;      // 16-byte groups per staged row
+  int lead;      // staged rows start `lead` pixels before the first window (TMA alignment)
   int left0;     // tw / 2
   int off;       // R - th + th / 2
   int BH;        // output rows per band
@@ -84,29 +111,24 @@ struct TensorParams {
 
 // Shared-memory layout, identical on host and device.
 struct Layout {
-  int raw_stage, raw, q_arr, q_stage, q, b_arr, b, pre, cum, stg, bars, total;
+  int row_bytes, raw_stage, raw, b_arr, b, rs, es, bars, total;
 };
 
 __host__ __device__ inline int align128(int x) { return (x + 127) & ~127; }
 
-__host__ __device__ inline Layout make_layout(int elem, int R, int K, int nblk, int boxw) {
+__host__ __device__ inline Layout make_layout(int elem, int R, int K, int nbox) {
   Layout L;
-  const int esz = elem == kF32 ? 4 : 1;
-  const int narr = elem == kF32 ? 2 : 1;
-  L.raw_stage = align128(kRawRows * boxw * esz);
+  L.row_bytes = nbox * 16;
+  L.raw_stage = align128(kRB * L.row_bytes);
   L.raw = 0;
-  L.q_arr = nblk * 128;
-  L.q_stage = align128(narr * L.q_arr + kM * 8);
-  L.q = L.raw + kNRaw * L.raw_stage;
-  L.b_arr = R * K * (elem == kF32 ? 2 : 1);
-  L.b = L.q + kNQ * L.q_stage;
-  L.pre = L.b + align128(narr * L.b_arr);
-  L.cum = L.pre + align128(2 * (boxw + 8) * 8);
-  L.stg = L.cum + R * kM * 8;
-  L.bars = L.stg + kG * kM * 16;
-  // mbarriers (2 per raw, operand and TMEM stage, plus one), then the TMEM
-  // address, the abort flag and the template energy.
-  L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNQ + 2 * kSTM + 1) + 32);
+  L.b_arr = 2 * R * K * (elem == kF32 ? 2 : 1);
+  L.b = L.raw + kNRaw * L.raw_stage;
+  L.rs = L.b + align128((elem == kF32 ? 2 : 1) * L.b_arr);
+  L.es = L.rs + R * kPos * 4;
+  L.bars = L.es + kNE * kPos * (elem == kF32 ? 8 : 4);
+  // mbarriers: raw full; ready and MMA done (4 each at most); energy full;
+  // done. Then the TMEM address, the abort flag and the template energy.
+  L.total = L.bars + align128(8 * (kNRaw + 2 * 4 + kNE + 1) + 32);
   return L;
 }
 
@@ -117,99 +139,81 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 __device__ __forceinline__ float bf16lo_f(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16hi_f(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
 
-// Row `rr` (0..7) of a BF16 core-matrix block: pixels rr..rr+7 of the 16
-// pixels held in w[0..3] (this lane's 8) and n[0..3] (the next lane's 8).
-template <int RR>
-__device__ __forceinline__ uint4 hankel_row_bf16(const uint32_t (&w)[4], const uint32_t (&n)[4]) {
-  uint32_t c[8] = {w[0], w[1], w[2], w[3], n[0], n[1], n[2], n[3]};
-  constexpr int a = RR / 2;
-  if (RR % 2 == 0) return make_uint4(c[a], c[a + 1], c[a + 2], c[a + 3]);
-  return make_uint4(__byte_perm(c[a], c[a + 1], 0x5432), __byte_perm(c[a + 1], c[a + 2], 0x5432),
-                    __byte_perm(c[a + 2], c[a + 3], 0x5432), __byte_perm(c[a + 3], c[a + 4], 0x5432));
-}
-
-// Row `rr` (0..7) of a U8 core-matrix block: bytes rr..rr+15 of the 24 bytes
-// in c[0..5].
-template <int RR>
-__device__ __forceinline__ uint4 hankel_row_u8(const uint32_t (&c)[6]) {
-  constexpr int a = RR / 4, sh = RR % 4;
-  constexpr uint32_t sel = sh == 1 ? 0x4321 : sh == 2 ? 0x5432 : 0x6543;
-  if (sh == 0) return make_uint4(c[a], c[a + 1], c[a + 2], c[a + 3]);
-  return make_uint4(__byte_perm(c[a], c[a + 1], sel), __byte_perm(c[a + 1], c[a + 2], sel),
-                    __byte_perm(c[a + 2], c[a + 3], sel), __byte_perm(c[a + 3], c[a + 4], sel));
-}
-
-template <int ELEM, int R>
+template <int ELEM, int R, int K>
 __global__ void __launch_bounds__(kThreads, 1)
     prox_tensor_kernel(const __grid_constant__ CUtensorMap tmap, const TensorParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  const Layout L = make_layout(ELEM, R, p.K, p.nblk, p.boxw);
-  constexpr int kTmemCols = (kSTM * R < 32) ? 32 : kSTM * R;
-  constexpr int ESZ = ELEM == kF32 ? 4 : 1;
+  const Layout L = make_layout(ELEM, R, K, p.nbox);
+  typedef Stages<ELEM, R, K> SG;
+  constexpr int N2 = SG::N2, AC = SG::AC, NS = SG::NS;
+  typedef typename std::conditional<ELEM == kF32, float, int>::type AT;   // accumulators
+  typedef typename std::conditional<ELEM == kF32, double, int>::type ET;  // window energy
 
+  // ready[i]: step t = i + k NS may be issued (its A operand is written and
+  //           the D stage of step t - NS has been read); 8 builder + 8
+  //           epilogue arrivals.
+  // mma_done[i]: the MMAs of step t have completed (D readable, A reusable).
   uint64_t* raw_full = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* raw_empty = raw_full + kNRaw;
-  uint64_t* q_full = raw_empty + kNRaw;
-  uint64_t* q_empty = q_full + kNQ;
-  uint64_t* tm_full = q_empty + kNQ;
-  uint64_t* tm_empty = tm_full + kSTM;
-  uint64_t* done_bar = tm_empty + kSTM;
+  uint64_t* ready = raw_full + kNRaw;
+  uint64_t* mma_done = ready + 4;
+  uint64_t* e_full = mma_done + 4;
+  uint64_t* done_bar = e_full + kNE;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   double* s_et = reinterpret_cast<double*>(tmem_slot + 2);
+  ET* estage = reinterpret_cast<ET*>(smem + L.es);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const bool need_e = p.measure != kCrossCorr;
-  const int xs_out = blockIdx.x * kM - p.xshift;
+  const int xs_out = blockIdx.x * kPos;  // strip b covers outputs [256 b, 256 b + 256)
   const int y0 = blockIdx.y * p.BH;
   const int yend = min(p.H, y0 + p.BH);
   const int r_begin = y0 - p.off;
   const int nsteps = (yend - y0) + R - 1;
+  const int nb = (nsteps + kRB - 1) / kRB;  // TMA loads (kRB rows each)
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kNRaw; ++i) {
-      mbar_init(&raw_full[i], 1);
-      mbar_init(&raw_empty[i], kRawRows);
+    for (int i = 0; i < kNRaw; ++i) mbar_init(&raw_full[i], 1);
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(&ready[i], kBuilders + kEpilogue);
+      mbar_init(&mma_done[i], 1);
     }
-    for (int i = 0; i < kNQ; ++i) {
-      mbar_init(&q_full[i], 1);
-      mbar_init(&q_empty[i], 1 + 4);
-    }
-    for (int i = 0; i < kSTM; ++i) {
-      mbar_init(&tm_full[i], 1);
-      mbar_init(&tm_empty[i], 4);
-    }
+    for (int i = 0; i < kNE; ++i) mbar_init(&e_full[i], kBuilders);
     mbar_init(done_bar, 1);
     *abort_flag = 0;
     fence_barrier_init();
+    // The first NS steps have no earlier D stage to wait for.
+    for (int i = 0; i < NS; ++i) mbar_arrive_n(&ready[i], kEpilogue);
   }
-  if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
+  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
 
-  // Template operand B (N = R rows, zero rows on top) and its energy.
+  // Template operand B (N2 = 2R rows: phase 0 then phase 1, zero rows on top
+  // of each) and the template energy.
   {
     const int padrows = R - p.th;
-    for (int idx = threadIdx.x; idx < R * p.K; idx += kThreads) {
-      const int n = idx / p.K, k = idx - n * p.K;
-      const int h = n - padrows;
+    for (int idx = threadIdx.x; idx < N2 * K; idx += kThreads) {
+      const int nn = idx / K, k = idx - nn * K;
+      const int ph = nn >= R ? 1 : 0;
+      const int h = nn - ph * R - padrows;
+      const int w = k - ph;
+      const bool in = h >= 0 && w >= 0 && w < p.tw;
       if (ELEM == kF32) {
         float t = 0.f;
-        if (h >= 0 && k < p.tw)
-          t = reinterpret_cast<const float*>(p.tmpl + (size_t)h * p.tmpl_pitch)[k];
+        if (in) t = reinterpret_cast<const float*>(p.tmpl + (size_t)h * p.tmpl_pitch)[w];
         const __nv_bfloat16 th_ = __float2bfloat16_rn(t);
         const __nv_bfloat16 tl_ = __float2bfloat16_rn(t - __bfloat162float(th_));
-        const int off = ((k >> 3) * R + n) * 16 + (k & 7) * 2;
+        const int off = ((k >> 3) * N2 + nn) * 16 + (k & 7) * 2;
         *reinterpret_cast<__nv_bfloat16*>(smem + L.b + off) = th_;
         *reinterpret_cast<__nv_bfloat16*>(smem + L.b + L.b_arr + off) = tl_;
       } else {
         uint8_t t = 0;
-        if (h >= 0 && k < p.tw)
-          t = reinterpret_cast<const uint8_t*>(p.tmpl + (size_t)h * p.tmpl_pitch)[k];
-        const int off = ((k >> 4) * R + n) * 16 + (k & 15);
+        if (in) t = reinterpret_cast<const uint8_t*>(p.tmpl + (size_t)h * p.tmpl_pitch)[w];
+        const int off = ((k >> 4) * N2 + nn) * 16 + (k & 15);
         smem[L.b + off] = t;
       }
     }
-    if (warp == 2) {
+    if (warp == 1) {
       double e = 0.0;
       for (int idx = lane; idx < p.th * p.tw; idx += 32) {
         const int h = idx / p.tw, k = idx - h * p.tw;
@@ -230,221 +234,267 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  constexpr uint32_t acol0 = NS * N2;  // first A column
 
-  if (warp == 0) {
-    // ---- TMA producer -------------------------------------------------------
+  const int sp = warp & 3;  // TMEM sub-partition of this warp
+  const int m = sp * 32 + lane;
+  const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(sp * 32) << 16);
+
+  if (warp == kBuilders + kEpilogue) {
+    // ---- Control: TMA loads of source rows, MMA issue ---------------------------
     if (lane == 0) {
       tma_prefetch_desc(&tmap);
-      const int nb = (nsteps + kRawRows - 1) / kRawRows;
-      const int xt = xs_out - p.left0;
+      // Staged row = pixels from xs_out - left0 - lead, a whole 16-byte group.
+      const int gx = (xs_out - p.left0 - p.lead) / p.inner;
       int issued = 0;
-      for (int b = 0; b < nb; ++b) {
-        const int st = b % kNRaw;
-        if (!mbar_wait(&raw_empty[st], ((b / kNRaw) & 1) ^ 1, abort_flag, kSpinLimit)) break;
-        mbar_arrive_expect_tx(&raw_full[st], kRawRows * p.boxw * ESZ);
-        tma_load_2d(smem + L.raw + st * L.raw_stage, &tmap, xt, r_begin + b * kRawRows,
-                    &raw_full[st]);
-        issued = b + 1;
+      for (; issued < min(nb, kNRaw); ++issued) {
+        mbar_arrive_expect_tx(&raw_full[issued], kRB * L.row_bytes);
+        tma_load_3d(smem + L.raw + issued * L.raw_stage, &tmap, 0, gx, r_begin + issued * kRB,
+                    &raw_full[issued]);
       }
-      // Every load this thread issued has landed before the CTA exits.
-      for (int b = max(0, issued - kNRaw); b < issued; ++b) {
-        volatile int no_abort = 0;
-        mbar_wait(&raw_full[b % kNRaw], (b / kNRaw) & 1, &no_abort, kSpinLimit);
-      }
-    }
-  } else if (warp == 1) {
-    // ---- MMA issuer -----------------------------------------------------------
-    if (lane == 0) {
-      const uint32_t q0 = smem_u32(smem + L.q);
       const uint32_t b0 = smem_u32(smem + L.b);
-      for (int s = 0; s < nsteps; ++s) {
-        const int qs = s % kNQ, ts = s % kSTM;
-        if (!mbar_wait(&q_full[qs], (s / kNQ) & 1, abort_flag, kSpinLimit)) break;
-        if (!mbar_wait(&tm_empty[ts], ((s / kSTM) & 1) ^ 1, abort_flag, kSpinLimit)) break;
-        tc_fence_after();
-        const uint32_t d = tmem_base + ts * R;
-        const uint32_t qa = q0 + qs * L.q_stage;
-        if (ELEM == kF32) {
-          constexpr uint32_t idesc = idesc_bf16_f32(kM, R);
-          const uint32_t qlo = qa + L.q_arr;
-          const uint32_t blo = b0 + L.b_arr;
-          const int nk = p.K / 16;
-          for (int kk = 0; kk < nk; ++kk)
-            mma_bf16(d, smem_desc(qa + kk * 256, 128, 128),
-                     smem_desc(b0 + kk * 2 * R * 16, R * 16, 128), idesc, kk > 0);
-          for (int kk = 0; kk < nk; ++kk)
-            mma_bf16(d, smem_desc(qa + kk * 256, 128, 128),
-                     smem_desc(blo + kk * 2 * R * 16, R * 16, 128), idesc, 1);
-          for (int kk = 0; kk < nk; ++kk)
-            mma_bf16(d, smem_desc(qlo + kk * 256, 128, 128),
-                     smem_desc(b0 + kk * 2 * R * 16, R * 16, 128), idesc, 1);
-        } else {
-          constexpr uint32_t idesc = idesc_u8_s32(kM, R);
-          const int nk = p.K / 32;
-          for (int kk = 0; kk < nk; ++kk)
-            mma_i8(d, smem_desc(qa + kk * 512, 256, 128),
-                   smem_desc(b0 + kk * 2 * R * 16, R * 16, 128), idesc, kk > 0);
+      int i = 0, st = 0, rr = 0;
+      uint32_t ph = 0;
+      for (int t = 0; t < nsteps; ++t) {
+        if (!mbar_wait(&ready[i], ph, abort_flag, kSpinLimit)) break;
+        // Every builder has read row t: its stage is free after the last row.
+        if (rr == kRB - 1 && issued < nb) {
+          mbar_arrive_expect_tx(&raw_full[st], kRB * L.row_bytes);
+          tma_load_3d(smem + L.raw + st * L.raw_stage, &tmap, 0, gx, r_begin + issued * kRB,
+                      &raw_full[st]);
+          ++issued;
         }
-        mma_commit(&tm_full[ts]);
-        mma_commit(&q_empty[qs]);
+        tc_fence_after();
+        const uint32_t d = tmem_base + i * N2;
+        const uint32_t a = tmem_base + acol0 + i * AC;
+        if (ELEM == kF32) {
+          constexpr uint32_t idesc = idesc_bf16_f32(kM, N2);
+          const uint32_t blo = b0 + L.b_arr;
+#pragma unroll
+          for (int kk = 0; kk < K / 16; ++kk)
+            mma_bf16_ts(d, a + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
+                        kk > 0);
+#pragma unroll
+          for (int kk = 0; kk < K / 16; ++kk)
+            mma_bf16_ts(d, a + kk * 8, smem_desc(blo + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
+                        1);
+#pragma unroll
+          for (int kk = 0; kk < K / 16; ++kk)
+            mma_bf16_ts(d, a + K / 2 + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128),
+                        idesc, 1);
+        } else {
+          constexpr uint32_t idesc = idesc_u8_s32(kM, N2);
+#pragma unroll
+          for (int kk = 0; kk < K / 32; ++kk)
+            mma_i8_ts(d, a + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
+                      kk > 0);
+        }
+        mma_commit(&mma_done[i]);
+        if (++i == NS) { i = 0; ph ^= 1; }
+        if (++rr == kRB) { rr = 0; if (++st == kNRaw) st = 0; }
       }
-      // Every MMA this thread issued has completed before TMEM is freed.
+      // Every MMA issued has completed before TMEM is freed, and every TMA
+      // load issued has landed before the CTA exits.
       mma_commit(done_bar);
       volatile int no_abort = 0;
       mbar_wait(done_bar, 0, &no_abort, kSpinLimit);
+      for (int b = max(0, issued - kNRaw); b < issued; ++b)
+        mbar_wait(&raw_full[b % kNRaw], (b / kNRaw) & 1, &no_abort, kSpinLimit);
     }
-  } else if (warp < 4) {
-    // ---- Hankel operand + row-energy builders ----------------------------------
-    const int pw = warp - 2;
-    double* pre = reinterpret_cast<double*>(smem + L.pre) + pw * (p.boxw + 8);
-    const int epl = (p.boxw + 31) / 32;
-    for (int s = pw; s < nsteps; s += 2) {
-      const int b = s / kRawRows, st = b % kNRaw, rr = s % kRawRows;
-      const int qs = s % kNQ;
-      if (!mbar_wait(&raw_full[st], (b / kNRaw) & 1, abort_flag, kSpinLimit)) break;
-      if (!mbar_wait(&q_empty[qs], ((s / kNQ) & 1) ^ 1, abort_flag, kSpinLimit)) break;
-      const unsigned char* row = smem + L.raw + st * L.raw_stage + rr * p.boxw * ESZ;
-      unsigned char* qst = smem + L.q + qs * L.q_stage;
-      const int t = lane;
+  } else if (warp < kBuilders) {
+    // ---- Builders: A operand of step t and the window energies ------------------
+    const int ph = warp >> 2;      // phase of the energies; K half of the A build
+    const int pos = 2 * m + ph;
+    float* rsring = reinterpret_cast<float*>(smem + L.rs);
+    ET ewin = ET(0);
+    int i = 0, st = 0, rr = 0;
+    uint32_t iph = 0, rph = 0;
+    for (int t = 0; t < nsteps; ++t) {
+      if (rr == 0 && !mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit)) break;
+      // A stage i is free once the MMAs of step t - NS have completed.
+      if (!mbar_wait(&mma_done[i], iph ^ 1, abort_flag, kSpinLimit)) break;
+      tc_fence_after();
+      const unsigned char* row = smem + L.raw + st * L.raw_stage + rr * L.row_bytes;
+      const uint32_t a_addr = lane_base + acol0 + i * AC;
+      float rsf = 0.f;
+      int rsi = 0;
       if (ELEM == kF32) {
-        uint32_t hi[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
-        if (t <= p.nblk) {
-          const float4 a = reinterpret_cast<const float4*>(row)[2 * t];
-          const float4 c = reinterpret_cast<const float4*>(row)[2 * t + 1];
-          const float f[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+        // This lane's window: pixels 2m .. 2m + K - 1 of the staged row, in
+        // chunks of 16 K columns. The chunks alternate between the two
+        // builders of a lane; both read every chunk when energies are needed.
+        // The window starts at pixel e0 = lead + 2m of the staged row; an odd
+        // e0 is read as aligned pairs from e0 - 1 and shifted by one.
+        const int e0 = p.lead + 2 * m;
+        const bool odd = e0 & 1;
+        const float2* r2 = reinterpret_cast<const float2*>(row) + (e0 >> 1);
+        float r0 = 0.f, r1 = 0.f;
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            hi[j] = pack_bf16(f[2 * j], f[2 * j + 1]);
-            lo[j] = pack_bf16(f[2 * j] - bf16lo_f(hi[j]), f[2 * j + 1] - bf16hi_f(hi[j]));
+        for (int c = 0; c < K / 16; ++c) {
+          const bool mine = (c & 1) == ph;
+          if (!mine && !need_e) continue;
+          float f[16];
+          if (odd) {
+            float prev = r2[c * 8].y;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const float2 v = r2[c * 8 + j + 1];
+              f[2 * j] = prev;
+              f[2 * j + 1] = v.x;
+              prev = v.y;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const float2 v = r2[c * 8 + j];
+              f[2 * j] = v.x;
+              f[2 * j + 1] = v.y;
+            }
+          }
+          if (mine) {
+            uint32_t hi[8], lo[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              hi[q] = pack_bf16(f[2 * q], f[2 * q + 1]);
+              lo[q] = pack_bf16(f[2 * q] - bf16lo_f(hi[q]), f[2 * q + 1] - bf16hi_f(hi[q]));
+            }
+            tmem_st8(a_addr + c * 8, hi);
+            tmem_st8(a_addr + K / 2 + c * 8, lo);
+          }
+          if (need_e) {
+            // Sum of squares over k in [ph, ph + tw). K = roundup16(tw + 1),
+            // so only k = 0 and the last chunk can fall outside.
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int k = c * 16 + j;
+              float v = f[j];
+              if (k == 0 || k >= K - 16) v = (k >= ph && k < ph + p.tw) ? v : 0.f;
+              if (j & 1)
+                r1 = fmaf(v, v, r1);
+              else
+                r0 = fmaf(v, v, r0);
+            }
           }
         }
-        uint32_t hn[4], ln[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          hn[j] = __shfl_down_sync(0xffffffffu, hi[j], 1);
-          ln[j] = __shfl_down_sync(0xffffffffu, lo[j], 1);
-        }
-        if (t < p.nblk) {
-          uint4* qh = reinterpret_cast<uint4*>(qst + t * 128);
-          uint4* ql = reinterpret_cast<uint4*>(qst + L.q_arr + t * 128);
-          qh[0] = hankel_row_bf16<0>(hi, hn); ql[0] = hankel_row_bf16<0>(lo, ln);
-          qh[1] = hankel_row_bf16<1>(hi, hn); ql[1] = hankel_row_bf16<1>(lo, ln);
-          qh[2] = hankel_row_bf16<2>(hi, hn); ql[2] = hankel_row_bf16<2>(lo, ln);
-          qh[3] = hankel_row_bf16<3>(hi, hn); ql[3] = hankel_row_bf16<3>(lo, ln);
-          qh[4] = hankel_row_bf16<4>(hi, hn); ql[4] = hankel_row_bf16<4>(lo, ln);
-          qh[5] = hankel_row_bf16<5>(hi, hn); ql[5] = hankel_row_bf16<5>(lo, ln);
-          qh[6] = hankel_row_bf16<6>(hi, hn); ql[6] = hankel_row_bf16<6>(lo, ln);
-          qh[7] = hankel_row_bf16<7>(hi, hn); ql[7] = hankel_row_bf16<7>(lo, ln);
-        }
+        rsf = r0 + r1;
       } else {
-        uint32_t w[2] = {0, 0};
-        if (t <= p.nblk + 1) {
-          const uint2 v = reinterpret_cast<const uint2*>(row)[t];
-          w[0] = v.x;
-          w[1] = v.y;
+        // Bytes e0 .. e0 + K - 1 (e0 = lead + 2m): words from the aligned
+        // base, shifted.
+        const int e0 = p.lead + 2 * m;
+        const uint32_t* r32 = reinterpret_cast<const uint32_t*>(row) + (e0 >> 2);
+        uint32_t w[K / 4 + 1];
+#pragma unroll
+        for (int j = 0; j <= K / 4; ++j) w[j] = r32[j];
+        const uint32_t sh = (e0 & 3) * 8;
+        uint32_t a[K / 4];
+#pragma unroll
+        for (int j = 0; j < K / 4; ++j) a[j] = __funnelshift_r(w[j], w[j + 1], sh);
+        // Each builder stores its half of the K/4 columns, 4 at a time.
+#pragma unroll
+        for (int c = 0; c < K / 16; ++c) {
+          if ((c & 1) == ph) tmem_st4(a_addr + c * 4, &a[c * 4]);
         }
-        uint32_t c[6];
-        c[0] = w[0];
-        c[1] = w[1];
-        c[2] = __shfl_down_sync(0xffffffffu, w[0], 1);
-        c[3] = __shfl_down_sync(0xffffffffu, w[1], 1);
-        c[4] = __shfl_down_sync(0xffffffffu, w[0], 2);
-        c[5] = __shfl_down_sync(0xffffffffu, w[1], 2);
-        if (t < p.nblk) {
-          uint4* q = reinterpret_cast<uint4*>(qst + t * 128);
-          q[0] = hankel_row_u8<0>(c);
-          q[1] = hankel_row_u8<1>(c);
-          q[2] = hankel_row_u8<2>(c);
-          q[3] = hankel_row_u8<3>(c);
-          q[4] = hankel_row_u8<4>(c);
-          q[5] = hankel_row_u8<5>(c);
-          q[6] = hankel_row_u8<6>(c);
-          q[7] = hankel_row_u8<7>(c);
+        if (need_e) {
+          const uint32_t sh2 = sh + 8 * ph;
+#pragma unroll
+          for (int j = 0; j < K / 4; ++j) {
+            const int rem = p.tw - 4 * j;
+            uint32_t v = __funnelshift_rc(w[j], w[j + 1], sh2);  // sh2 may be 32
+            if (rem <= 0) v = 0;
+            else if (rem < 4) v &= (1u << (8 * rem)) - 1u;
+            rsi = static_cast<int>(__dp4a(v, v, static_cast<unsigned>(rsi)));
+          }
         }
       }
       if (need_e) {
-        // Prefix sums of S^2 over the staged row, then the row-window sums
-        // rs[m] = sum_{w < tw} S(m + w)^2 for the 128 positions.
-        double run = 0.0;
-        double vals[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int j = lane * epl + k;
-          double v = 0.0;
-          if (k < epl && j < p.boxw) {
-            v = ELEM == kF32 ? (double)reinterpret_cast<const float*>(row)[j]
-                             : (double)row[j];
-            v = v * v;
-          }
-          run += v;
-          vals[k] = run;
+        // Window energy: add this row, drop the row th steps back (the ring
+        // holds R >= th rows; read before write when th == R).
+        float* slot = rsring + (t & (R - 1)) * kPos + pos;
+        const float* oslot = rsring + ((t - p.th) & (R - 1)) * kPos + pos;
+        if (ELEM == kF32) {
+          const float old = t >= p.th ? *oslot : 0.f;
+          *slot = rsf;
+          ewin += static_cast<ET>((double)rsf - (double)old);
+        } else {
+          const int old = t >= p.th ? __float_as_int(*oslot) : 0;
+          *slot = __int_as_float(rsi);
+          ewin += static_cast<ET>(rsi - old);
         }
-        double incl = run;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const double o = __shfl_up_sync(0xffffffffu, incl, d);
-          if (lane >= d) incl += o;
-        }
-        const double excl = incl - run;
-        if (lane == 0) pre[0] = 0.0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int j = lane * epl + k;
-          if (k < epl && j < p.boxw) pre[j + 1] = excl + vals[k];
-        }
-        __syncwarp();
-        double* rs = reinterpret_cast<double*>(qst + (ELEM == kF32 ? 2 : 1) * L.q_arr);
-#pragma unroll
-        for (int j = 0; j < kM / 32; ++j) {
-          const int m = lane + 32 * j;
-          rs[m] = pre[m + p.tw] - pre[m];
-        }
+        estage[(t & (kNE - 1)) * kPos + pos] = ewin;
       }
-      fence_async_smem();
+      tmem_st_wait();
+      tc_fence_before();
       __syncwarp();
       if (lane == 0) {
-        mbar_arrive(&raw_empty[st]);
-        mbar_arrive(&q_full[qs]);
+        if (need_e) mbar_arrive(&e_full[t & (kNE - 1)]);
+        mbar_arrive(&ready[i]);
       }
+      if (++i == NS) { i = 0; iph ^= 1; }
+      if (++rr == kRB) { rr = 0; if (++st == kNRaw) { st = 0; rph ^= 1; } }
     }
   } else {
-    // ---- Epilogue: ring accumulation, window energy, output -----------------------
-    const int ew = warp - 4;
-    const int m = ew * 32 + lane;
-    const int x = xs_out + m;
+    // ---- Epilogue: running sums over template rows, energies, output ------------
+    const int ph = (warp - kBuilders) >> 2;  // positions 2m + ph, D columns [ph R, ph R + R)
+    const int pos = 2 * m + ph;
+    const int x = xs_out + pos;
     const bool x_ok = (x >= 0 && x < p.W);
-    // U8: exact integers carried in double (the s32 MMA results and their sums
-    // stay far below 2^53).
-    typedef typename std::conditional<ELEM == kF32, float, double>::type AT;
     AT acc[R];
 #pragma unroll
-    for (int i = 0; i < R; ++i) acc[i] = AT(0);
-    double cum = 0.0;
-    double* cumring = reinterpret_cast<double*>(smem + L.cum);
-    const double et = *s_et;
-    const uint32_t lane_addr = tmem_base + (static_cast<uint32_t>(ew * 32) << 16);
-    AT* stage_v = reinterpret_cast<AT*>(smem + L.stg);
-    double* stage_e = reinterpret_cast<double*>(smem + L.stg + kG * kM * 8);
-    // Output of the completed rows staged in shared memory (kG steps at a
-    // time): keeps the unrolled ring loop small.
-    auto flush = [&](int sbase, int cnt) {
-#pragma unroll 1
-      for (int j = 0; j < cnt; ++j) {
-        const int yd = r_begin + sbase + j + p.off - R + 1;
-        if (yd < y0 || yd >= yend || !x_ok) continue;
-        const AT a = stage_v[j * kM + m];
-        const double e = stage_e[j * kM + m];
+    for (int j = 0; j < R; ++j) acc[j] = AT(0);
+    const ET et = static_cast<ET>(*s_et);
+    const double etd = *s_et;
+    int i = 0;
+    uint32_t iph = 0;
+    for (int s = 0; s < nsteps; ++s) {
+      if (!mbar_wait(&mma_done[i], iph, abort_flag, kSpinLimit)) break;
+      tc_fence_after();
+      // D[n] = column i*N2 + ph*R + n. Chunks are taken from the top so the
+      // shift-add below runs with ascending c (acc[c - 1] <- acc[c] + D[R-1-c]).
+      constexpr int CW = R == 32 ? 32 : 16;  // 16-column loads keep R = 64 in registers
+      AT outv = AT(0);
+#pragma unroll
+      for (int q = R / CW - 1; q >= 0; --q) {
+        uint32_t v[32];
+        if (CW == 32)
+          tmem_ld32(lane_base + i * N2 + ph * R + q * CW, v);
+        else
+          tmem_ld16(lane_base + i * N2 + ph * R + q * CW, v);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = CW - 1; j >= 0; --j) {
+          const int n = q * CW + j;
+          const int c = R - 1 - n;
+          const AT val = ELEM == kF32 ? (AT)__uint_as_float(v[j]) : (AT) static_cast<int>(v[j]);
+          if (c == 0)
+            outv = acc[0] + val;
+          else
+            acc[c - 1] = acc[c] + val;
+        }
+      }
+      acc[R - 1] = AT(0);
+      ET e = ET(0);
+      if (need_e) {
+        if (!mbar_wait(&e_full[s & (kNE - 1)], (s / kNE) & 1, abort_flag, kSpinLimit)) break;
+        e = estage[(s & (kNE - 1)) * kPos + pos];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ready[i]);  // D stage i free for step s + NS
+      if (++i == NS) { i = 0; iph ^= 1; }
+
+      const int yd = y0 + s - R + 1;
+      if (s >= R - 1 && yd < yend && x_ok) {
         double outd;
         float outf;
         if (ELEM == kF32) {
-          const double cc = (double)a;
+          const double cc = (double)outv;
+          const double ed = (double)e;
           if (p.measure == kCrossCorr) outd = cc;
-          else if (p.measure == kSqrDistance) outd = e - 2.0 * cc + et;
-          else if (p.measure == kCrossCorrNorm) outd = __ddiv_rn(cc, __dsqrt_rn(__dmul_rn(e, et)));
-          else outd = __ddiv_rn(e - 2.0 * cc + et, __dsqrt_rn(__dmul_rn(e, et)));
+          else if (p.measure == kSqrDistance) outd = ed - 2.0 * cc + etd;
+          else if (p.measure == kCrossCorrNorm) outd = cc * rsqrt(ed * etd);
+          else outd = (ed - 2.0 * cc + etd) * rsqrt(ed * etd);
           outf = (float)outd;
         } else {
-          const long long cc = (long long)a;
+          const long long cc = (long long)outv;
           const long long es = (long long)e, ei = (long long)et;
           const long long num =
               (p.measure == kCrossCorr || p.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
@@ -465,71 +515,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         else
           reinterpret_cast<float*>(o)[x] = outf;
       }
-    };
-    bool ok = true;
-    for (int s0 = 0; s0 < nsteps && ok; s0 += R) {
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        const int s = s0 + i;
-        if (s >= nsteps || !ok) break;
-        const int ts = s % kSTM, qs = s % kNQ;
-        if (!mbar_wait(&tm_full[ts], (s / kSTM) & 1, abort_flag, kSpinLimit)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-#pragma unroll
-        for (int c = 0; c < (R + 31) / 32; ++c) {
-          uint32_t v[32];
-          if (R >= 32)
-            tmem_ld32(lane_addr + ts * R + c * 32, v);
-          else
-            tmem_ld16(lane_addr + ts * R, v);
-          tmem_ld_wait();
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int n = c * 32 + j;
-            if (n < R) {
-              if (ELEM == kF32)
-                acc[(i - n + R) % R] += __uint_as_float(v[j]);
-              else
-                acc[(i - n + R) % R] += (double)static_cast<int>(v[j]);
-            }
-          }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tm_empty[ts]);
-        double e = 0.0;
-        if (need_e) {
-          if (!mbar_wait(&q_full[qs], (s / kNQ) & 1, abort_flag, kSpinLimit)) {
-            ok = false;
-            break;
-          }
-          const double* rs =
-              reinterpret_cast<const double*>(smem + L.q + qs * L.q_stage +
-                                              (ELEM == kF32 ? 2 : 1) * L.q_arr);
-          cum += rs[m];
-          const double old = (s >= p.th) ? cumring[((s - p.th) % R) * kM + m] : 0.0;
-          cumring[(s % R) * kM + m] = cum;
-          e = cum - old;
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&q_empty[qs]);
-        const int g = i % kG;
-        const int slot = (i + 1) % R;
-        stage_v[g * kM + m] = acc[slot];
-        stage_e[g * kM + m] = e;
-        acc[slot] = AT(0);
-        if (g == kG - 1) flush(s - (kG - 1), kG);
-      }
     }
-    if (ok && (nsteps % kG) != 0) flush(nsteps - nsteps % kG, nsteps % kG);
   }
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 1) {
+  if (warp == 0) {
     tc_fence_after();
     tmem_dealloc(tmem_base, kTmemCols);
   }
@@ -556,7 +547,25 @@ EncodeTiledFn encode_fn() {
 
 int ring_size(int th) { return th <= 16 ? 16 : th <= 32 ? 32 : 64; }
 
-template <int ELEM, int R>
+// Band height: the fewest waves of CTAs times the steps per band (output
+// rows plus the R - 1 rows of ramp), over all band counts.
+int band_height(int H, int R, int nstrips, int sm_count) {
+  long long best = LLONG_MAX;
+  int best_bh = H;
+  for (int nb = 1; nb <= std::max(1, H / 8); ++nb) {
+    const int bh = (H + nb - 1) / nb;
+    const int nbe = (H + bh - 1) / bh;
+    const long long waves = (static_cast<long long>(nstrips) * nbe + sm_count - 1) / sm_count;
+    const long long cost = waves * (bh + R - 1);
+    if (cost < best) {
+      best = cost;
+      best_bh = bh;
+    }
+  }
+  return best_bh;
+}
+
+template <int ELEM, int R, int K>
 cudaError_t launch_elem(Context& ctx, Measure m, const DevImage& src, const DevImage& tmpl,
                         const DevImage& dst) {
   TensorParams p;
@@ -564,14 +573,14 @@ cudaError_t launch_elem(Context& ctx, Measure m, const DevImage& src, const DevI
   p.H = src.height;
   p.tw = tmpl.width;
   p.th = tmpl.height;
-  p.K = ELEM == kF32 ? (p.tw + 15) / 16 * 16 : (p.tw + 31) / 32 * 32;
-  p.nblk = ELEM == kF32 ? 15 + p.K / 8 : 14 + p.K / 8;
-  p.boxw = kM + p.K;
+  p.inner = ELEM == kF32 ? 4 : 16;
+  // Lane m reads pixels lead + 2m .. lead + 2m + K (one more for odd leads).
+  p.nbox = (kPos + K + 2 * p.inner + 1) / p.inner;
   p.left0 = p.tw / 2;
-  const int align = ELEM == kF32 ? 4 : 16;
-  p.xshift = ((p.left0 % align) == 0) ? 0 : align - (p.left0 % align);
+  p.lead = (p.inner - p.left0 % p.inner) % p.inner;
   p.off = R - p.th + p.th / 2;
-  p.BH = p.H >= 2048 ? 512 : std::max(64, (p.H + 3) / 4);
+  const int nstrips = (p.W + kPos - 1) / kPos;
+  p.BH = band_height(p.H, R, nstrips, ctx.sm_count);
   p.measure = m;
   p.norm_float = (double)p.tw * p.th * 65025.0 <= 16777216.0;
   p.tmpl = (const char*)tmpl.ptr;
@@ -583,36 +592,63 @@ cudaError_t launch_elem(Context& ctx, Measure m, const DevImage& src, const DevI
 
   EncodeTiledFn enc = encode_fn();
   if (!enc) return cudaErrorNotSupported;
+  // Rank-3 view of the source: 16-byte groups (dim 0), groups along the row
+  // (dim 1), rows (dim 2). A staged row of 256 + K pixels is one box of
+  // nbox groups, under the 256-element box limit. The last group of a row may
+  // reach into the row pitch, which image creation zero-fills.
   CUtensorMap map;
-  const cuuint64_t gdim[2] = {(cuuint64_t)p.W, (cuuint64_t)p.H};
-  const cuuint64_t gstride[1] = {(cuuint64_t)src.pitch};
-  const cuuint32_t box[2] = {(cuuint32_t)p.boxw, (cuuint32_t)kRawRows};
-  const cuuint32_t estride[2] = {1, 1};
+  const cuuint64_t gdim[3] = {(cuuint64_t)p.inner, (cuuint64_t)((p.W + p.inner - 1) / p.inner),
+                              (cuuint64_t)p.H};
+  const cuuint64_t gstride[2] = {16, (cuuint64_t)src.pitch};
+  const cuuint32_t box[3] = {(cuuint32_t)p.inner, (cuuint32_t)p.nbox, (cuuint32_t)kRB};
+  const cuuint32_t estride[3] = {1, 1, 1};
   CUresult r = enc(&map, ELEM == kF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
-                   2, src.ptr, gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   3, src.ptr, gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
 
-  const Layout L = make_layout(ELEM, R, p.K, p.nblk, p.boxw);
-  auto kern = prox_tensor_kernel<ELEM, R>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
+  const Layout L = make_layout(ELEM, R, K, p.nbox);
+  const int smem_bytes = std::max(L.total, kMinSmem);
+  auto kern = prox_tensor_kernel<ELEM, R, K>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   if (e != cudaSuccess) return e;
-  const int nstrips = (p.W + p.xshift + kM - 1) / kM;
   const int nbands = (p.H + p.BH - 1) / p.BH;
   dim3 grid(nstrips, nbands, 1);
-  kern<<<grid, kThreads, L.total, ctx.stream>>>(map, p);
+  kern<<<grid, kThreads, smem_bytes, ctx.stream>>>(map, p);
   count_launches(1);
   return cudaGetLastError();
+}
+
+template <int ELEM, int R>
+cudaError_t launch_k(Context& ctx, Measure m, const DevImage& s, const DevImage& t,
+                     const DevImage& d) {
+  const int tw = t.width;
+  if constexpr (ELEM == kF32) {
+    switch ((tw + 1 + 15) / 16) {
+      case 1: return launch_elem<ELEM, R, 16>(ctx, m, s, t, d);
+      case 2: return launch_elem<ELEM, R, 32>(ctx, m, s, t, d);
+      case 3: return launch_elem<ELEM, R, 48>(ctx, m, s, t, d);
+      case 4: return launch_elem<ELEM, R, 64>(ctx, m, s, t, d);
+      default: return launch_elem<ELEM, R, 80>(ctx, m, s, t, d);
+    }
+  } else {
+    switch ((tw + 1 + 31) / 32) {
+      case 1: return launch_elem<ELEM, R, 32>(ctx, m, s, t, d);
+      case 2: return launch_elem<ELEM, R, 64>(ctx, m, s, t, d);
+      default: return launch_elem<ELEM, R, 96>(ctx, m, s, t, d);
+    }
+  }
 }
 
 template <int ELEM>
 cudaError_t launch_r(Context& ctx, Measure m, const DevImage& s, const DevImage& t,
                      const DevImage& d) {
   switch (ring_size(t.height)) {
-    case 16: return launch_elem<ELEM, 16>(ctx, m, s, t, d);
-    case 32: return launch_elem<ELEM, 32>(ctx, m, s, t, d);
-    default: return launch_elem<ELEM, 64>(ctx, m, s, t, d);
+    case 16: return launch_k<ELEM, 16>(ctx, m, s, t, d);
+    case 32: return launch_k<ELEM, 32>(ctx, m, s, t, d);
+    default: return launch_k<ELEM, 64>(ctx, m, s, t, d);
   }
 }
 
