@@ -4,11 +4,13 @@ Bars:
   * U8 sources (i8 MMA, exact s32 sums, exact window statistics): results are
     bit-identical to the plain path, which equals the reference wherever the
     reference's float sums are exact;
-  * F32 sources (split BF16 hi/lo, three MMAs, FP64 window statistics):
-    relative error <= 1e-5 against the long-double oracle for CrossCorr and
-    CrossCorr_Norm; SqrDistance[_Norm] (which cancel to 0 at a match) within
-    1e-5 of the scale of their terms, sum S^2 + sum T^2 of the window
-    (divided by sqrt(sum S^2 * sum T^2) for the _Norm form).
+  * F32 and U16 sources (split BF16 hi/lo, three MMAs, FP64 window
+    statistics): relative error <= 1e-5 against the long-double oracle for
+    CrossCorr and CrossCorr_Norm; SqrDistance[_Norm] (which cancel to 0 at a
+    match) within 1e-5 of the scale of their terms, sum S^2 + sum T^2 of the
+    window (divided by sqrt(sum S^2 * sum T^2) for the _Norm form);
+  * 2-4 channel sources: the same bars per channel (the channels are split
+    into planes and run as one launch).
 """
 import numpy as np
 import pytest
@@ -33,9 +35,10 @@ def f32_check(got, S, T, m):
         # SqrDistance[_Norm] cancel to 0 at a match: error relative to the
         # scale of the terms, (sum S^2 + sum T^2) [/ sqrt(sum S^2 * sum T^2)].
         ss, _, tt = O.window_terms_exact(S, T)
-        scale = ss + tt[0]
+        tt = tt if S.ndim == 3 else tt[0]
+        scale = ss + tt
         if m == 1:
-            scale = scale / np.sqrt(ss * tt[0])
+            scale = scale / np.sqrt(ss * tt)
         fin = np.isfinite(scale)
         err = np.abs(got[fin] - ex[fin]) / np.maximum(scale[fin], 1e-30)
     else:
@@ -130,8 +133,9 @@ def test_f32_signed_values(ocip, ctx):
 
 
 def test_fallbacks_to_plain(ocip, ctx):
-    """AbsDistance, multi-channel and large templates are served by the plain
-    path even when the tensor path is requested."""
+    """AbsDistance, types without a tensor form, small F32 templates and large
+    templates are served by the plain path even when the tensor path is
+    requested."""
     ctx.make_current()
     rng = np.random.default_rng(5)
     S = rng.random((80, 90)).astype(np.float32)
@@ -140,6 +144,15 @@ def test_fallbacks_to_plain(ocip, ctx):
     assert path == ocip.PATH_PLAIN
     S4 = rng.random((40, 50, 4)).astype(np.float32)
     _, path = run(ocip, ctx, 3, S4, rng.random((5, 5, 4)).astype(np.float32), ocip.PATH_TENSOR)
+    assert path == ocip.PATH_PLAIN
+    Si16 = rng.integers(-100, 100, (40, 50), dtype=np.int16)
+    _, path = run(ocip, ctx, 3, Si16, rng.integers(-9, 9, (9, 9), dtype=np.int16),
+                  ocip.PATH_TENSOR)
+    assert path == ocip.PATH_PLAIN
+    # AUTO keeps U16 (split, not exact) on the plain path
+    S16 = rng.integers(0, 65535, (40, 50), dtype=np.uint16)
+    _, path = run(ocip, ctx, 3, S16, rng.integers(0, 65535, (9, 9), dtype=np.uint16),
+                  ocip.PATH_AUTO)
     assert path == ocip.PATH_PLAIN
     _, path = run(ocip, ctx, 3, rng.random((100, 100)).astype(np.float32),
                   rng.random((65, 65)).astype(np.float32), ocip.PATH_TENSOR)
@@ -161,4 +174,103 @@ def test_f64_destination(ocip, ctx):
     got, path = run(ocip, ctx, 0, S, T, ocip.PATH_TENSOR, out_dtype=np.float64)
     assert path == ocip.PATH_TENSOR
     assert np.array_equal(got, O.proximity_exact(0, S, T))
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+@pytest.mark.parametrize("nch", [2, 3, 4])
+@pytest.mark.parametrize("th,tw", [(16, 16), (31, 31), (64, 64), (5, 40)])
+def test_u8_multichannel_tensor_equals_plain(ocip, ctx, nch, th, tw):
+    ctx.make_current()
+    rng = np.random.default_rng(nch * 1000 + th * 10 + tw)
+    S = rng.integers(0, 256, (90, 300, nch), dtype=np.uint8)
+    T = rng.integers(0, 256, (th, tw, nch), dtype=np.uint8)
+    for m in (0, 1, 3, 4):
+        plain, p1 = run(ocip, ctx, m, S, T, ocip.PATH_PLAIN)
+        tens, p2 = run(ocip, ctx, m, S, T, ocip.PATH_AUTO)
+        assert p1 == ocip.PATH_PLAIN and p2 == ocip.PATH_TENSOR
+        assert np.array_equal(plain, tens, equal_nan=True), (MEAS[m], nch)
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+@pytest.mark.parametrize("nch", [1, 4])
+@pytest.mark.parametrize("th,tw", [(31, 31), (64, 64), (12, 40), (40, 12)])
+def test_u16_tensor_accuracy(ocip, ctx, nch, th, tw):
+    ctx.make_current()
+    rng = np.random.default_rng(nch * 100 + th + tw)
+    shape = (70, 270, nch) if nch > 1 else (70, 270)
+    tshape = (th, tw, nch) if nch > 1 else (th, tw)
+    S = rng.integers(0, 65536, shape, dtype=np.uint16)
+    T = rng.integers(0, 65536, tshape, dtype=np.uint16)
+    for m in (0, 1, 3, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert path == ocip.PATH_TENSOR
+        f32_check(got, S, T, m)
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+@pytest.mark.parametrize("nch", [3, 4])
+def test_f32_multichannel_accuracy(ocip, ctx, nch):
+    ctx.make_current()
+    rng = np.random.default_rng(nch)
+    S = rng.random((80, 290, nch)).astype(np.float32)
+    T = rng.random((20, 24, nch)).astype(np.float32)
+    for m in (0, 1, 3, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert path == ocip.PATH_TENSOR
+        f32_check(got, S, T, m)
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def cfg5_images(dtype):
+    """3840x2160x4 field as in the multi-channel config: uniform noise plus a
+    blob field (U8), or the field scaled to 0-65535 (U16); 64x64x4 template
+    cut at a seeded offset."""
+    import bench
+    rng = np.random.default_rng(55)
+    field = np.stack([bench.blob_field(3840, 2160, nblobs=60, seed=60 + c) for c in range(4)], -1)
+    field = field / field.max()
+    if dtype == np.uint8:
+        S = np.clip(rng.integers(0, 128, field.shape) + 127 * field, 0, 255).astype(np.uint8)
+    else:
+        S = np.round(field * 65535).astype(np.uint16)
+    y, x = 700, 1900
+    return S, S[y:y + 64, x:x + 64].copy()
+
+
+def test_cfg5_u8_full_size_tensor_equals_plain(ocip, ctx):
+    """Full-size 3840x2160x4 U8, 64x64x4 template: the tensor path's _Norm maps
+    are bit-identical to the plain path's (exact integer sums on both)."""
+    ctx.make_current()
+    S, T = cfg5_images(np.uint8)
+    for m in (1, 4):
+        plain, _ = run(ocip, ctx, m, S, T, ocip.PATH_PLAIN)
+        tens, path = run(ocip, ctx, m, S, T, ocip.PATH_AUTO)
+        assert path == ocip.PATH_TENSOR
+        assert np.array_equal(plain, tens, equal_nan=True), MEAS[m]
+    ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_cfg5_u16_full_size_accuracy_on_crops(ocip, ctx):
+    """Full-size 3840x2160x4 U16 on the tensor path, checked against the
+    long-double oracle on crops (interior, corner and edges)."""
+    ctx.make_current()
+    S, T = cfg5_images(np.uint16)
+    for m in (1, 4):
+        got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+        assert path == ocip.PATH_TENSOR
+        for (y, x) in [(700, 1900), (0, 0), (2160 - 48, 3840 - 48), (1000, 0)]:
+            # the window of output (y..y+n, x..x+n) needs 64 rows/cols around it
+            y0, x0 = max(0, y - 64), max(0, x - 64)
+            y1, x1 = min(2160, y + 48 + 64), min(3840, x + 48 + 64)
+            crop_ex = O.proximity_exact(m, S[y0:y1, x0:x1], T)
+            sub = got[y:y + 48, x:x + 48]
+            ex = crop_ex[y - y0:y - y0 + 48, x - x0:x - x0 + 48]
+            # crop borders only where the crop is the image border
+            if m == 1:
+                ss, _, tt = O.window_terms_exact(S[y0:y1, x0:x1], T)
+                scale = ((ss + tt) / np.sqrt(ss * tt))[y - y0:y - y0 + 48, x - x0:x - x0 + 48]
+                err = np.abs(sub - ex) / scale
+            else:
+                err = np.abs(sub - ex) / np.abs(ex)
+            assert err.max() <= TOL, (MEAS[m], y, x, err.max())
     ctx.set_path(ocip.PATH_PLAIN)
