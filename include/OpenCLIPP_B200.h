@@ -17,9 +17,10 @@ extern "C" {
  *                     (the drop-in default).
  *   OCIP_PATH_TENSOR: tcgen05 tensor cores for the product term of
  *                     SqrDistance[_Norm] and CrossCorr[_Norm] (i8 MMA with exact
- *                     s32 sums for 8-bit sources, split BF16 for F32) with
- *                     FP64/int64 window statistics; AbsDistance and shapes
- *                     the tensor kernels do not cover fall back to PLAIN.
+ *                     s32 sums for U8 sources, split BF16 for F32 and U16;
+ *                     1-4 channels; templates up to 64 x 64) with FP64/int32
+ *                     window statistics; AbsDistance and shapes the tensor
+ *                     kernels do not cover fall back to PLAIN.
  *   OCIP_PATH_AUTO  : TENSOR where it is exact (8-bit sources), PLAIN
  *                     otherwise. */
 enum ocipProximityPath {
@@ -63,6 +64,45 @@ ocipError ocip_API ocipGetLaunchCount(uint64_t* Count);
 ocipError ocip_API ocipIntegralNoAlloc(int Square, SImage SourceDesc, const void* Source,
                                        size_t SourcePitch, SImage DestDesc, void* Dest,
                                        size_t DestPitch, void* Stream);
+
+/* Measures, for the batched calls below. */
+enum ocipMeasure {
+  OCIP_MEASURE_SQR_DISTANCE = 0,
+  OCIP_MEASURE_SQR_DISTANCE_NORM = 1,
+  OCIP_MEASURE_ABS_DISTANCE = 2,
+  OCIP_MEASURE_CROSS_CORR = 3,
+  OCIP_MEASURE_CROSS_CORR_NORM = 4,
+};
+
+/* Batched template matching. No reference counterpart: the reference matches
+ * one (image, template) pair per call.
+ * Prepares one persistent launch that computes Measure for every pair:
+ *   Dests[i * NbTemplates + j] = Measure(Images[i], Templates[j])
+ * with the same definition, zero padding and Dest types as the one-pair calls.
+ * All images and templates share one type (U8, U16 or F32) and channel count
+ * (1-4); templates are at most 64 x 64 and no larger than any image; each
+ * Dest is F32 or F64 with its image's size and channels. AbsDistance has no
+ * tensor-core form and is refused (CL_INVALID_VALUE). The work is a queue of
+ * (pair, channel, 256-column strip, band of rows) items, largest first,
+ * taken by one persistent CTA per SM on the tensor path (U8 exact; F32 and
+ * U16 within 1e-5 relative). Band heights are chosen per (template size
+ * class, type, channels) by timing candidates on the device the first time a
+ * class is seen in the process. The queue reset and the launch are captured
+ * in a CUDA graph that ocipRunProximityBatch replays on the context's stream.
+ * Images and templates with host data are uploaded here; the batch reads
+ * their device buffers when it runs, so later changes must be sent with
+ * ocipSendImage. Dests are marked as written. Release with ocipReleaseProgram;
+ * the images must outlive the program. */
+ocipError ocip_API ocipPrepareProximityBatch(ocipProgram* Program, int Measure,
+                                             const ocipImage* Images, int NbImages,
+                                             const ocipImage* Templates, int NbTemplates,
+                                             const ocipImage* Dests);
+ocipError ocip_API ocipRunProximityBatch(ocipProgram Program);
+/* Work items of a prepared batch, and the band height (rows per item) it
+ * uses for templates of the given size (0 if the batch has none). */
+ocipError ocip_API ocipGetProximityBatchInfo(ocipProgram Program, int TemplateWidth,
+                                             int TemplateHeight, int* NbItems,
+                                             int* BandHeight);
 
 /* Device address and row pitch (bytes) of an image's device buffer. */
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,

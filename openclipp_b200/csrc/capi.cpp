@@ -20,6 +20,7 @@
 #include "../../include/OpenCLIPP_B200.h"
 #include "host.h"
 #include "internal.h"
+#include "tensor.h"
 
 using namespace ocipb;
 
@@ -271,6 +272,7 @@ ocipError ocipReleaseImage(ocipImage h) {
 ocipError ocipReleaseProgram(ocipProgram h) {
   Program* p = reinterpret_cast<Program*>(h);
   if (p != nullptr && p->magic == Program::kMagic) {
+    if (p->batch) tensor_batch_destroy(p->batch);
     if (p->scratch) {
       if (g_contexts.count(p->ctx)) {
         cudaSetDevice(p->ctx->device);

@@ -66,12 +66,13 @@ struct Image {
 // buffers (Integral: C++/programs/Integral.cpp:42-95).
 struct Program {
   static constexpr uint32_t kMagic = 0x0C1F9E0Au;
-  enum Kind { kIntegral = 1, kProximityFFT = 2 };
+  enum Kind { kIntegral = 1, kProximityFFT = 2, kProximityBatch = 3 };
   uint32_t magic = kMagic;
   int kind = kIntegral;
   Context* ctx = nullptr;
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  struct TensorBatch* batch = nullptr;  // kProximityBatch
 };
 
 extern thread_local std::string g_last_error;

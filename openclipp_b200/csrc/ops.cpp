@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/OpenCLIPP.h"
 #include "../../include/OpenCLIPP_B200.h"
@@ -195,10 +196,91 @@ void integral(bool sqr, ocipProgram hp, ocipImage hs, ocipImage hd) {
   D.in_device = true;
 }
 
+// Batched matching (extension, no reference counterpart): the checks of the
+// one-pair calls for every pair, plus what the tensor path needs.
+void batch_prepare(ocipProgram* out, int measure, const ocipImage* himgs, int nimg,
+                   const ocipImage* htpls, int ntpl, const ocipImage* hdsts) {
+  Context& ctx = current();
+  if (out == nullptr) fail(CL_INVALID_VALUE, "Program is NULL");
+  if (measure < 0 || measure > kCrossCorrNorm || measure == kAbsDistance)
+    fail(CL_INVALID_VALUE, "measure not available in batches (AbsDistance has no product form)");
+  if (nimg <= 0 || ntpl <= 0 || himgs == nullptr || htpls == nullptr || hdsts == nullptr)
+    fail(CL_INVALID_VALUE, "empty batch");
+  std::vector<Image*> imgs, tpls, dsts;
+  for (int i = 0; i < nimg; ++i) imgs.push_back(&image(himgs[i]));
+  for (int j = 0; j < ntpl; ++j) tpls.push_back(&image(htpls[j]));
+  for (int k = 0; k < nimg * ntpl; ++k) dsts.push_back(&image(hdsts[k]));
+  for (Image* x : imgs) same_context(ctx, *x);
+  for (Image* x : tpls) same_context(ctx, *x);
+  for (Image* x : dsts) same_context(ctx, *x);
+  const Image& first = *imgs[0];
+  for (Image* x : imgs)
+    if (!same_type(first, *x)) fail(CL_INVALID_VALUE, "batch images must share type and channels");
+  for (int i = 0; i < nimg; ++i) {
+    const Image& S = *imgs[i];
+    for (int j = 0; j < ntpl; ++j) {
+      const Image& T = *tpls[j];
+      const Image& D = *dsts[i * ntpl + j];
+      if (T.desc.Width > S.desc.Width || T.desc.Height > S.desc.Height)
+        fail(CL_INVALID_VALUE, "Template image must be smaller than the source image.");
+      if (!same_type(S, T)) fail(CL_INVALID_VALUE, "Source and Template must have same type.");
+      if (S.desc.Width != D.desc.Width || S.desc.Height != D.desc.Height)
+        fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+      if (S.desc.Channels != D.desc.Channels)
+        fail(CL_INVALID_VALUE, "Different number of channels used");
+      if (!type_is_float((int)D.desc.Type))
+        fail(CL_INVALID_VALUE, "non-float image used when not allowed");
+      if (!tensor_supports((Measure)measure, dev_view(S), dev_view(T), dev_view(D), true))
+        fail(CL_INVALID_VALUE,
+             "batches run on the tensor path: U8, U16 or F32 sources, templates of 64 x 64 "
+             "or less (F32 and U16: at least 64 pixels)");
+    }
+  }
+  for (Image* x : imgs) send_if_needed(*x);
+  for (Image* x : tpls) send_if_needed(*x);
+  std::vector<DevImage> vi, vt, vd;
+  for (Image* x : imgs) vi.push_back(dev_view(*x));
+  for (Image* x : tpls) vt.push_back(dev_view(*x));
+  for (Image* x : dsts) vd.push_back(dev_view(*x));
+  cudaError_t e = cudaSuccess;
+  TensorBatch* b = tensor_batch_create(ctx, (Measure)measure, vi, vt, vd, &e);
+  check_cuda(e, "batch preparation");
+  Program* p = new Program();
+  p->kind = Program::kProximityBatch;
+  p->ctx = &ctx;
+  p->batch = b;
+  for (Image* x : dsts) x->in_device = true;
+  *out = reinterpret_cast<ocipProgram>(p);
+}
+
 }  // namespace
 }  // namespace ocipb
 
 extern "C" {
+
+ocipError ocipPrepareProximityBatch(ocipProgram* Program, int Measure, const ocipImage* Images,
+                                    int NbImages, const ocipImage* Templates, int NbTemplates,
+                                    const ocipImage* Dests) {
+  OCIP_GUARD(batch_prepare(Program, Measure, Images, NbImages, Templates, NbTemplates, Dests))
+}
+
+ocipError ocipRunProximityBatch(ocipProgram P) {
+  OCIP_GUARD(
+    Context& ctx = current();
+    ocipb::Program& prog = program(P, ocipb::Program::kProximityBatch);
+    if (prog.ctx != &ctx) fail(CL_INVALID_CONTEXT, "program belongs to another context");
+    check_cuda(tensor_batch_run(prog.batch), "batch launch");
+  )
+}
+
+ocipError ocipGetProximityBatchInfo(ocipProgram P, int TemplateWidth, int TemplateHeight,
+                                    int* NbItems, int* BandHeight) {
+  OCIP_GUARD(
+    ocipb::Program& prog = program(P, ocipb::Program::kProximityBatch);
+    if (NbItems) *NbItems = tensor_batch_items(prog.batch);
+    if (BandHeight) *BandHeight = tensor_batch_band_height(prog.batch, TemplateWidth, TemplateHeight);
+  )
+}
 
 ocipError ocipPrepareProximity(ocipImage Image) {
   OCIP_GUARD(

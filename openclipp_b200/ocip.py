@@ -96,6 +96,13 @@ def _load():
         "ocipGetLaunchCount": (i32, [ctypes.POINTER(ctypes.c_uint64)]),
         "ocipIntegralNoAlloc": (i32, [ctypes.c_int, SImage, vp, ctypes.c_size_t, SImage, vp,
                                       ctypes.c_size_t, vp]),
+        "ocipPrepareProximityBatch": (i32, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp),
+                                            ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
+                                            ctypes.POINTER(vp)]),
+        "ocipRunProximityBatch": (i32, [vp]),
+        "ocipGetProximityBatchInfo": (i32, [vp, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -286,6 +293,42 @@ class Program:
         if self.handle:
             lib.ocipReleaseProgram(self.handle)
             self.handle = ctypes.c_void_p()
+
+
+MEASURE_INDEX = {"SqrDistance": 0, "SqrDistance_Norm": 1, "AbsDistance": 2, "CrossCorr": 3,
+                 "CrossCorr_Norm": 4}
+
+
+class Batch(Program):
+    """A prepared batch (ocipPrepareProximityBatch): measure of every
+    (image i, template j) pair into dests[i * len(templates) + j]."""
+
+    def __init__(self, measure, images, templates, dests):
+        n, m = len(images), len(templates)
+        arr = lambda xs: (ctypes.c_void_p * len(xs))(*[x.handle for x in xs])
+        self._keep = (arr(images), arr(templates), arr(dests))
+        h = ctypes.c_void_p()
+        code = measure if isinstance(measure, int) else MEASURE_INDEX[measure]
+        rc = lib.ocipPrepareProximityBatch(ctypes.byref(h), code, self._keep[0], n,
+                                           self._keep[1], m, self._keep[2])
+        super().__init__(h)
+        self.rc = rc
+
+    def run(self):
+        return lib.ocipRunProximityBatch(self.handle)
+
+    def info(self, tw=0, th=0):
+        """(work items, band height used for tw x th templates)."""
+        n, bh = ctypes.c_int(), ctypes.c_int()
+        check(lib.ocipGetProximityBatchInfo(self.handle, tw, th, ctypes.byref(n), ctypes.byref(bh)),
+              "ocipGetProximityBatchInfo")
+        return n.value, bh.value
+
+
+def prepare_batch(measure, images, templates, dests):
+    b = Batch(measure, images, templates, dests)
+    check(b.rc, "ocipPrepareProximityBatch")
+    return b
 
 
 def prepare_integral(img=None):
