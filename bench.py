@@ -564,6 +564,106 @@ def run_batch_bench(args, world, rank, local):
     }
 
 
+def run_backward_bench(args, world, rank, local):
+    """Differentiation workload: 32 F32 images of 1024x1024 (blob field), each
+    with a 32x32 template (its seeded crop + N(0, 0.02)). Forward =
+    CrossCorr_Norm and SqrDistance of every pair; backward = the gradients of
+    sum G1 SqrDistance + sum G2 CrossCorr_Norm (G ~ N(0, 1)) with respect to
+    the image and the template. Reports both times and their ratio."""
+    import torch
+
+    from openclipp_b200 import ocip
+    n_img, side, ts = 32, 1024, 32
+    rng = np.random.default_rng(41)
+    ctx = ocip.Context(local)
+    ctx.set_path(ocip.PATH_TENSOR)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    imgs, tps, g1s, g2s, sqs, ccs, dss, dts = [], [], [], [], [], [], [], []
+    for k in range(rank, n_img, world):
+        S = blob_field(side, side, nblobs=60, seed=400 + k)
+        y, x = (int(v) for v in rng.integers(0, side - ts, 2))
+        T = (S[y:y + ts, x:x + ts] + rng.normal(0, 0.02, (ts, ts))).astype(np.float32)
+        imgs.append(ocip.Image(S))
+        tps.append(ocip.Image(T))
+        g1s.append(ocip.Image(rng.standard_normal((side, side)).astype(np.float32)))
+        g2s.append(ocip.Image(rng.standard_normal((side, side)).astype(np.float32)))
+        sqs.append(ocip.Image(shape=(side, side), dtype=np.float32))
+        ccs.append(ocip.Image(shape=(side, side), dtype=np.float32))
+        dss.append(ocip.Image(shape=(side, side), dtype=np.float32))
+        dts.append(ocip.Image(shape=(ts, ts), dtype=np.float32))
+    for x in imgs + tps + g1s + g2s:
+        x.send()
+
+    def forward():
+        for i in range(len(imgs)):
+            ocip.check(ocip.sqr_distance(imgs[i], tps[i], sqs[i]), "fwd")
+            ocip.check(ocip.cross_corr_norm(imgs[i], tps[i], ccs[i]), "fwd")
+
+    def backward():
+        for i in range(len(imgs)):
+            ocip.check(ocip.proximity_backward(imgs[i], tps[i], g1s[i], g2s[i], ccs[i], dss[i],
+                                               dts[i]), "bwd")
+
+    def timed(fn, n):
+        out = []
+        for _ in range(n):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    for _ in range(args.warmup):
+        forward()
+        backward()
+    torch.cuda.synchronize()
+    barrier()
+    with Clocks(local) as clk:
+        f_ms = allreduce_max(float(np.mean(timed(forward, args.steps))))
+        b_ms = allreduce_max(float(np.mean(timed(backward, args.steps))))
+    taps = n_img * (side - ts + 1) ** 2 * ts * ts  # per measure, valid region
+    # Gradient check on a crop of the first pair against the long-double adjoint.
+    from oracle import oracle as O
+    crop = np.ascontiguousarray(blob_field(side, side, nblobs=60, seed=400 + rank)[:192, :192])
+    rng2 = np.random.default_rng(3)
+    Tc = (crop[40:72, 60:92] + rng2.normal(0, 0.02, (ts, ts))).astype(np.float32)
+    G1 = rng2.standard_normal(crop.shape).astype(np.float32)
+    G2 = rng2.standard_normal(crop.shape).astype(np.float32)
+    Ci, Ti = ocip.Image(crop), ocip.Image(Tc)
+    N = np.zeros(crop.shape, np.float32)
+    Ni = ocip.Image(N)
+    ocip.check(ocip.cross_corr_norm(Ci, Ti, Ni), "fwd")
+    dS = np.zeros(crop.shape, np.float32)
+    dT = np.zeros((ts, ts), np.float32)
+    G1i, G2i, dSi, dTi = ocip.Image(G1), ocip.Image(G2), ocip.Image(dS), ocip.Image(dT)
+    ocip.check(ocip.proximity_backward(Ci, Ti, G1i, G2i, Ni, dSi, dTi), "bwd")
+    dSi.read()
+    dTi.read()
+    a0, b0 = O.proximity_backward(0, crop, Tc, G1)
+    a4, b4 = O.proximity_backward(4, crop, Tc, G2)
+    err_s = float(np.abs(dS - (a0 + a4)).max() / np.abs(a0 + a4).max())
+    err_t = float(np.abs(dT - (b0 + b4)).max() / np.abs(b0 + b4).max())
+    for x in imgs + tps + g1s + g2s + sqs + ccs + dss + dts + [Ci, Ti, Ni, G1i, G2i, dSi, dTi]:
+        x.release()
+    ctx.close()
+    return {
+        "metric": "backward / forward time, CrossCorr_Norm + SqrDistance (tensor path)",
+        "value": round(b_ms / f_ms, 3), "unit": "ratio", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(b_ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded blob fields, templates cut with N(0, 0.02) noise)",
+        "config": {"workload": f"{n_img} x {side}x{side} F32 images, {ts}x{ts} templates; "
+                               "forward = SqrDistance + CrossCorr_Norm, backward = dS and dT "
+                               "of both in one pass"},
+        "forward_ms": round(f_ms, 3), "backward_ms": round(b_ms, 3),
+        "forward_gtaps": round(2 * taps * world / (f_ms * 1e-3) / 1e9, 1),
+        "adjoint_rel_err_vs_fp64": {"dS": err_s, "dT": err_t},
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,9 +676,10 @@ def main():
     ap.add_argument("--measures", default=",".join(MEASURES),
                     help="comma-separated subset of the five measures (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm (profiling)")
-    ap.add_argument("--workload", choices=["single", "batch"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "backward"], default="single",
                     help="single: 4096^2 F32, 31x31, five measures (the headline); batch: 16 x "
-                         "2048^2 U8 x 64 uneven templates in persistent launches")
+                         "2048^2 U8 x 64 uneven templates in persistent launches; backward: "
+                         "32 x 1024^2 F32 with 32x32 templates, gradients vs forward time")
     args = ap.parse_args()
     args.measures = [m for m in args.measures.split(",") if m]
     assert all(m in MEASURES for m in args.measures), args.measures
@@ -593,6 +694,8 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "batch":
         res = run_batch_bench(args, world, rank, local)
+    elif args.workload == "backward":
+        res = run_backward_bench(args, world, rank, local)
     else:
         res = run_ours(args, world, rank, local)
     if rank == 0:

@@ -104,6 +104,27 @@ ocipError ocip_API ocipGetProximityBatchInfo(ocipProgram Program, int TemplateWi
                                              int TemplateHeight, int* NbItems,
                                              int* BandHeight);
 
+/* Gradients of template matching (no reference counterpart).
+ * For L = sum_{x,y} GradSqrDistance(x,y) * SqrDistance(Source, Template)(x,y)
+ *       + sum_{x,y} GradCrossCorrNorm(x,y) * CrossCorr_Norm(Source, Template)(x,y)
+ * writes dL/dSource into GradSource and dL/dTemplate into GradTemplate, with
+ * the forward definitions of ocipSqrDistance and ocipCrossCorr_Norm (window
+ * anchored at (tw/2, th/2), zero padding; padded pixels receive no gradient).
+ * Source and Template are F32 with one channel, the template at most 64 x 64.
+ * GradSqrDistance and GradCrossCorrNorm are F32 maps of the source's size;
+ * either may be NULL (but not both). CrossCorrNorm is the forward
+ * ocipCrossCorr_Norm map (F32), required with GradCrossCorrNorm; the window
+ * energies are recomputed, not stored. GradSource (source size) and
+ * GradTemplate (template size) are F32 or F64; either may be NULL. Positions
+ * whose window energy is 0 (CrossCorr_Norm undefined) contribute nothing.
+ * Both measures are served by one pass: a correlation of an adjoint map with
+ * the flipped template and a template-gradient reduction, both on the tensor
+ * cores (split BF16), with FP64 window sums. */
+ocipError ocip_API ocipProximityBackward(ocipImage Source, ocipImage Template,
+                                         ocipImage GradSqrDistance, ocipImage GradCrossCorrNorm,
+                                         ocipImage CrossCorrNorm, ocipImage GradSource,
+                                         ocipImage GradTemplate);
+
 /* Device address and row pitch (bytes) of an image's device buffer. */
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,
                                          size_t* Pitch);

@@ -253,10 +253,74 @@ void batch_prepare(ocipProgram* out, int measure, const ocipImage* himgs, int ni
   *out = reinterpret_cast<ocipProgram>(p);
 }
 
+void backward(ocipImage hs, ocipImage ht, ocipImage hg1, ocipImage hg2, ocipImage hn2,
+              ocipImage hds, ocipImage hdt) {
+  Context& ctx = current();
+  Image& S = image(hs);
+  Image& T = image(ht);
+  same_context(ctx, S);
+  same_context(ctx, T);
+  auto f32_1ch = [](const Image& x) {
+    return x.desc.Type == SImage::F32 && x.desc.Channels == 1;
+  };
+  auto same_size = [](const Image& a, const Image& b) {
+    return a.desc.Width == b.desc.Width && a.desc.Height == b.desc.Height;
+  };
+  if (!f32_1ch(S) || !f32_1ch(T))
+    fail(CL_INVALID_VALUE, "backward: Source and Template must be F32 with one channel");
+  if (T.desc.Width > S.desc.Width || T.desc.Height > S.desc.Height)
+    fail(CL_INVALID_VALUE, "Template image must be smaller than the source image.");
+  if (T.desc.Width > 64 || T.desc.Height > 64)
+    fail(CL_INVALID_VALUE, "backward: templates up to 64 x 64");
+  if (hg1 == nullptr && hg2 == nullptr)
+    fail(CL_INVALID_VALUE, "backward: no upstream gradient");
+  Image* G1 = hg1 ? &image(hg1) : nullptr;
+  Image* G2 = hg2 ? &image(hg2) : nullptr;
+  Image* N2 = hn2 ? &image(hn2) : nullptr;
+  Image* dS = hds ? &image(hds) : nullptr;
+  Image* dT = hdt ? &image(hdt) : nullptr;
+  if (G2 && !N2) fail(CL_INVALID_VALUE, "backward: CrossCorrNorm map needed with its gradient");
+  for (Image* x : {G1, G2, N2}) {
+    if (!x) continue;
+    same_context(ctx, *x);
+    if (!f32_1ch(*x)) fail(CL_INVALID_VALUE, "backward: gradient maps must be F32, one channel");
+    if (!same_size(*x, S)) fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  }
+  for (Image* x : {dS, dT}) {
+    if (!x) continue;
+    same_context(ctx, *x);
+    if (!type_is_float((int)x->desc.Type) || x->desc.Channels != 1)
+      fail(CL_INVALID_VALUE, "backward: gradients are written as F32 or F64, one channel");
+  }
+  if (dS && !same_size(*dS, S)) fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  if (dT && !same_size(*dT, T)) fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  for (Image* x : {&S, &T, G1, G2, N2})
+    if (x) send_if_needed(*x);
+  DevImage vg1, vg2, vn2, vds, vdt;
+  if (G1) vg1 = dev_view(*G1);
+  if (G2) vg2 = dev_view(*G2);
+  if (N2) vn2 = dev_view(*N2);
+  if (dS) vds = dev_view(*dS);
+  if (dT) vdt = dev_view(*dT);
+  check_cuda(proximity_backward(ctx, dev_view(S), dev_view(T), G1 ? &vg1 : nullptr,
+                                G2 ? &vg2 : nullptr, N2 ? &vn2 : nullptr, dS ? &vds : nullptr,
+                                dT ? &vdt : nullptr),
+             "backward launch");
+  if (dS) dS->in_device = true;
+  if (dT) dT->in_device = true;
+}
+
 }  // namespace
 }  // namespace ocipb
 
 extern "C" {
+
+ocipError ocipProximityBackward(ocipImage Source, ocipImage Template, ocipImage GradSqrDistance,
+                                ocipImage GradCrossCorrNorm, ocipImage CrossCorrNorm,
+                                ocipImage GradSource, ocipImage GradTemplate) {
+  OCIP_GUARD(backward(Source, Template, GradSqrDistance, GradCrossCorrNorm, CrossCorrNorm,
+                      GradSource, GradTemplate))
+}
 
 ocipError ocipPrepareProximityBatch(ocipProgram* Program, int Measure, const ocipImage* Images,
                                     int NbImages, const ocipImage* Templates, int NbTemplates,

@@ -115,6 +115,7 @@ struct ItemArgs {
   const CUtensorMap* tmap;  // source planes (rank 4: group, groups, rows, channel)
   int W, H;
   int tw, th;
+  int ax, ay;    // window anchor: output (x, y) reads S(x + w - ax, y + h - ay)
   int nch, ch;
   int xs_out;    // strip covers outputs [xs_out, xs_out + 256)
   int y0, yend;  // band of output rows
@@ -247,11 +248,11 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   const int lane = threadIdx.x & 31;
   const bool need_e = a.measure != kCrossCorr;
   const int ch = a.ch;
-  const int left0 = a.tw / 2;
+  const int left0 = a.ax;
   // Staged rows start `lead` pixels before the strip's first window pixel,
   // at a whole 16-byte group (TMA alignment).
   const int lead = (TR::inner - left0 % TR::inner) % TR::inner;
-  const int off = R - a.th + a.th / 2;
+  const int off = R - a.th + a.ay;
   const int r_begin = a.y0 - off;
   const int nsteps = (a.yend - a.y0) + R - 1;
   const int nb = (nsteps + kRB - 1) / kRB;  // TMA loads (kRB rows each)
@@ -731,6 +732,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.H = im.H;
           item.tw = tp.tw;
           item.th = tp.th;
+          item.ax = tp.tw / 2;
+          item.ay = tp.th / 2;
           item.nch = im.nch;
           item.ch = bi.ch;
           item.xs_out = bi.strip * kPos;
@@ -880,7 +883,7 @@ int smem_for_class(int cls, int nbox) {
 
 template <int ELEM>
 cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevImage& tmpl,
-                       const DevImage& dst) {
+                       const DevImage& dst, int ax, int ay) {
   const int cls = class_of<ELEM>(tmpl.width, tmpl.height);
   int R, K;
   class_rk<ELEM>(cls, &R, &K);
@@ -898,6 +901,8 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
   a.H = src.height;
   a.tw = tmpl.width;
   a.th = tmpl.height;
+  a.ax = ax;
+  a.ay = ay;
   a.nch = src.nch;
   a.nbox = P.nbox;
   a.tmpl = (const char*)tmpl.ptr;
@@ -1267,9 +1272,16 @@ bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl, const
 
 cudaError_t launch_proximity_tensor(Context& ctx, Measure m, const DevImage& src,
                                     const DevImage& tmpl, const DevImage& dst) {
-  if (src.type == U8) return launch_one<kU8>(ctx, m, src, tmpl, dst);
-  if (src.type == U16) return launch_one<kU16>(ctx, m, src, tmpl, dst);
-  return launch_one<kF32>(ctx, m, src, tmpl, dst);
+  return launch_proximity_tensor_anchored(ctx, m, src, tmpl, dst, tmpl.width / 2,
+                                          tmpl.height / 2);
+}
+
+cudaError_t launch_proximity_tensor_anchored(Context& ctx, Measure m, const DevImage& src,
+                                             const DevImage& tmpl, const DevImage& dst, int ax,
+                                             int ay) {
+  if (src.type == U8) return launch_one<kU8>(ctx, m, src, tmpl, dst, ax, ay);
+  if (src.type == U16) return launch_one<kU16>(ctx, m, src, tmpl, dst, ax, ay);
+  return launch_one<kF32>(ctx, m, src, tmpl, dst, ax, ay);
 }
 
 TensorBatch* tensor_batch_create(Context& ctx, Measure m, const std::vector<DevImage>& imgs,

@@ -17,6 +17,21 @@ bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl,
 cudaError_t launch_proximity_tensor(Context& ctx, Measure m, const DevImage& src,
                                     const DevImage& tmpl, const DevImage& dst);
 
+// Same with a general window anchor: output (x, y) reads
+// S(x + w - ax, y + h - ay) (the one-pair calls use ax = tw/2, ay = th/2).
+// 0 <= ax < tw, 0 <= ay < th.
+cudaError_t launch_proximity_tensor_anchored(Context& ctx, Measure m, const DevImage& src,
+                                             const DevImage& tmpl, const DevImage& dst, int ax,
+                                             int ay);
+
+// Gradients of L = sum G1 * SqrDistance(S, T) + sum G2 * CrossCorr_Norm(S, T)
+// (F32 sources, one channel, templates up to 64 x 64) into dS (S's size) and
+// dT (T's size), F32 or F64; G1 or G2 may be null, N2 is CrossCorr_Norm(S, T)
+// (needed with G2), dS or dT may be null.
+cudaError_t proximity_backward(Context& ctx, const DevImage& S, const DevImage& T,
+                               const DevImage* G1, const DevImage* G2, const DevImage* N2,
+                               const DevImage* dS, const DevImage* dT);
+
 // A prepared batch: every (image i, template j) pair into dsts[i * ntpl + j],
 // one persistent launch over a work queue of (pair, channel, strip, band)
 // items, captured in a CUDA graph. All images share one type; every pair must

@@ -100,6 +100,7 @@ def _load():
                                             ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int,
                                             ctypes.POINTER(vp)]),
         "ocipRunProximityBatch": (i32, [vp]),
+        "ocipProximityBackward": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "ocipGetProximityBatchInfo": (i32, [vp, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
@@ -329,6 +330,13 @@ def prepare_batch(measure, images, templates, dests):
     b = Batch(measure, images, templates, dests)
     check(b.rc, "ocipPrepareProximityBatch")
     return b
+
+
+def proximity_backward(S, T, G1=None, G2=None, N2=None, dS=None, dT=None):
+    """ocipProximityBackward on Image handles (None for absent ones); returns
+    the error code."""
+    h = lambda x: x.handle if x is not None else None
+    return lib.ocipProximityBackward(h(S), h(T), h(G1), h(G2), h(N2), h(dS), h(dT))
 
 
 def prepare_integral(img=None):
