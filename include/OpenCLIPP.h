@@ -151,6 +151,26 @@ ocipError ocip_API ocipIntegral(ocipProgram Program, ocipImage Source,
 ocipError ocip_API ocipSqrIntegral(ocipProgram Program, ocipImage Source,
                                    ocipImage Dest);
 
+/* ---- Statistics: arg-min / arg-max of a map (reference
+ * include/OpenCLIPP.h:544-563; only the index reductions, the consumers of a
+ * score map, are provided) ------------------------------------------------ */
+/* Program for the statistics calls; Image may be NULL. */
+ocipError ocip_API ocipPrepareStatistics(ocipProgram* ProgramPtr, ocipImage Image);
+
+/* Minimum (maximum; of the absolute values for the Abs forms) of a one-channel
+ * image and the coordinate of a pixel that holds it. Synchronous. Value,
+ * position and tie-breaking are the reference's: the minimum as a float, the
+ * first such pixel in the reference's reduction order. More than one channel
+ * gives CL_INVALID_VALUE. */
+ocipError ocip_API ocipMinIndx(ocipProgram Program, ocipImage Source, double* Result,
+                               int* IndexX, int* IndexY);
+ocipError ocip_API ocipMaxIndx(ocipProgram Program, ocipImage Source, double* Result,
+                               int* IndexX, int* IndexY);
+ocipError ocip_API ocipMinAbsIndx(ocipProgram Program, ocipImage Source, double* Result,
+                                  int* IndexX, int* IndexY);
+ocipError ocip_API ocipMaxAbsIndx(ocipProgram Program, ocipImage Source, double* Result,
+                                  int* IndexX, int* IndexY);
+
 /* ---- Image proximity (reference include/OpenCLIPP.h:649-669) ----------- */
 /* Dest has the size and channel count of Source and a float type (F32; F64
  * sources compute in double). The window of Dest(x, y) covers Source

@@ -125,6 +125,17 @@ ocipError ocip_API ocipProximityBackward(ocipImage Source, ocipImage Template,
                                          ocipImage CrossCorrNorm, ocipImage GradSource,
                                          ocipImage GradTemplate);
 
+/* Every wait in the tensor-core kernels is bounded: when one expires (about 2 s
+ * of SM clock), the kernel sets an error flag and returns instead of hanging,
+ * and the next ocipFinish or ocipReadImage of the context returns
+ * CL_OUT_OF_RESOURCES (the results since the previous such call are not
+ * valid); the context stays usable.
+ * This diagnostic runs that path on purpose: a kernel waits on a barrier that
+ * nothing arrives on for LimitCycles SM clock cycles (at most 2^31 - 1). It
+ * returns what ocipFinish returns afterwards: CL_OUT_OF_RESOURCES when the
+ * bounded wait expired as designed. */
+ocipError ocip_API ocipTestBoundedWait(int LimitCycles);
+
 /* Device address and row pitch (bytes) of an image's device buffer. */
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,
                                          size_t* Pitch);

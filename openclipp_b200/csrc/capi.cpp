@@ -94,8 +94,23 @@ void* Context::scratch(int slot, size_t bytes) {
     }
     check_cuda(cudaMalloc(&s.ptr, bytes), "scratch allocation");
     s.bytes = bytes;
+    // New scratch starts zeroed: the kernels' error flag lives in one slot.
+    check_cuda(cudaMemsetAsync(s.ptr, 0, bytes, stream), "scratch initialisation");
   }
   return s.ptr;
+}
+
+void Context::check_device_errors() {
+  const Scratch& s = scratch_[kTensorAux];
+  if (s.ptr == nullptr) return;
+  int flag = 0;
+  check_cuda(cudaMemcpy(&flag, s.ptr, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+  if (flag) {
+    check_cuda(cudaMemset(s.ptr, 0, sizeof(int)), "error flag");
+    fail(CL_OUT_OF_RESOURCES,
+         "a tensor-core kernel gave up a bounded wait; results since the last ocipFinish or "
+         "ocipReadImage are not valid");
+  }
 }
 
 Context::~Context() {
@@ -192,6 +207,7 @@ ocipError ocipFinish(void) {
   OCIP_GUARD(
     Context& ctx = current();
     check_cuda(cudaStreamSynchronize(ctx.stream), "ocipFinish");
+    ctx.check_device_errors();
   )
 }
 
@@ -252,6 +268,7 @@ ocipError ocipReadImage(ocipImage h) {
                                  cudaMemcpyDeviceToHost, ctx.stream),
                "read image");
     check_cuda(cudaStreamSynchronize(ctx.stream), "read image");
+    ctx.check_device_errors();
   )
 }
 

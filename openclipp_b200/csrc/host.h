@@ -35,6 +35,11 @@ struct Context {
   int path = 1;       // ocipProximityPath; PLAIN by default (the drop-in)
   int last_path = 1;  // path that served the last proximity call
   void* scratch(int slot, size_t bytes);
+  // The tensor-path kernels set a device flag (kTensorAux scratch) when a
+  // bounded wait expires (the kernel then returns without finishing its
+  // work). Called after the stream is synchronised: clears the flag and fails
+  // with CL_OUT_OF_RESOURCES if it was set.
+  void check_device_errors();
   ~Context();
 
  private:
@@ -66,7 +71,7 @@ struct Image {
 // buffers (Integral: C++/programs/Integral.cpp:42-95).
 struct Program {
   static constexpr uint32_t kMagic = 0x0C1F9E0Au;
-  enum Kind { kIntegral = 1, kProximityFFT = 2, kProximityBatch = 3 };
+  enum Kind { kIntegral = 1, kProximityFFT = 2, kProximityBatch = 3, kStatistics = 4 };
   uint32_t magic = kMagic;
   int kind = kIntegral;
   Context* ctx = nullptr;

@@ -19,6 +19,7 @@
 #include "../../include/OpenCLIPP_B200.h"
 #include "host.h"
 #include "internal.h"
+#include "statistics.h"
 #include "tensor.h"
 
 using namespace ocipb;
@@ -310,10 +311,61 @@ void backward(ocipImage hs, ocipImage ht, ocipImage hg1, ocipImage hg2, ocipImag
   if (dT) dT->in_device = true;
 }
 
+// Statistics::Min/Max/MinAbs/MaxAbs with coordinates
+// (C++/programs/Statistics.cpp:244-298): one channel only (Check1Channel,
+// C++/programs/Program.cpp:501-505), synchronous.
+void index_op(int op, ocipProgram hp, ocipImage hs, double* result, int* x, int* y) {
+  Context& ctx = current();
+  Program& prog = program(hp, Program::kStatistics);
+  if (prog.ctx != &ctx) fail(CL_INVALID_CONTEXT, "program belongs to another context");
+  Image& S = image(hs);
+  same_context(ctx, S);
+  if (S.desc.Channels > 1) fail(CL_INVALID_VALUE, "only 1 channel images are allowed");
+  if (result == nullptr || x == nullptr || y == nullptr) fail(CL_INVALID_VALUE, "NULL result");
+  const size_t need = index_reduce_scratch_bytes((int)S.desc.Width, (int)S.desc.Height);
+  if (prog.scratch_bytes < need) {
+    if (prog.scratch) {
+      check_cuda(cudaStreamSynchronize(ctx.stream), "statistics scratch sync");
+      cudaFree(prog.scratch);
+      prog.scratch = nullptr;
+      prog.scratch_bytes = 0;
+    }
+    check_cuda(cudaMalloc(&prog.scratch, need), "statistics scratch allocation");
+    prog.scratch_bytes = need;
+  }
+  send_if_needed(S);
+  check_cuda(index_reduce(ctx, op, dev_view(S), prog.scratch, result, x, y), "index reduction");
+  ctx.check_device_errors();
+}
+
 }  // namespace
 }  // namespace ocipb
 
 extern "C" {
+
+ocipError ocipPrepareStatistics(ocipProgram* ProgramPtr, ocipImage Img) {
+  OCIP_GUARD(
+    Context& ctx = current();
+    if (ProgramPtr == nullptr) fail(CL_INVALID_VALUE, "ProgramPtr is NULL");
+    if (Img != nullptr) image(Img);
+    Program* p = new Program();
+    p->kind = Program::kStatistics;
+    p->ctx = &ctx;
+    *ProgramPtr = reinterpret_cast<ocipProgram>(p);
+  )
+}
+ocipError ocipMinIndx(ocipProgram P, ocipImage S, double* R, int* X, int* Y) {
+  OCIP_GUARD(index_op(kIdxMin, P, S, R, X, Y))
+}
+ocipError ocipMaxIndx(ocipProgram P, ocipImage S, double* R, int* X, int* Y) {
+  OCIP_GUARD(index_op(kIdxMax, P, S, R, X, Y))
+}
+ocipError ocipMinAbsIndx(ocipProgram P, ocipImage S, double* R, int* X, int* Y) {
+  OCIP_GUARD(index_op(kIdxMinAbs, P, S, R, X, Y))
+}
+ocipError ocipMaxAbsIndx(ocipProgram P, ocipImage S, double* R, int* X, int* Y) {
+  OCIP_GUARD(index_op(kIdxMaxAbs, P, S, R, X, Y))
+}
 
 ocipError ocipProximityBackward(ocipImage Source, ocipImage Template, ocipImage GradSqrDistance,
                                 ocipImage GradCrossCorrNorm, ocipImage CrossCorrNorm,
@@ -326,6 +378,16 @@ ocipError ocipPrepareProximityBatch(ocipProgram* Program, int Measure, const oci
                                     int NbImages, const ocipImage* Templates, int NbTemplates,
                                     const ocipImage* Dests) {
   OCIP_GUARD(batch_prepare(Program, Measure, Images, NbImages, Templates, NbTemplates, Dests))
+}
+
+ocipError ocipTestBoundedWait(int LimitCycles) {
+  OCIP_GUARD(
+    Context& ctx = current();
+    if (LimitCycles <= 0) fail(CL_INVALID_VALUE, "LimitCycles must be positive");
+    check_cuda(launch_bounded_wait_probe(ctx, LimitCycles), "bounded-wait probe");
+    check_cuda(cudaStreamSynchronize(ctx.stream), "bounded-wait probe");
+    ctx.check_device_errors();
+  )
 }
 
 ocipError ocipRunProximityBatch(ocipProgram P) {

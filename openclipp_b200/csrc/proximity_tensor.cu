@@ -1256,6 +1256,33 @@ TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& 
 
 }  // namespace
 
+namespace {
+
+// One thread waits on an mbarrier that nothing arrives on, with the bounded
+// wait of the tensor kernels: the wait expires, sets the abort flag, and the
+// kernel raises the context's error flag and returns.
+__global__ void bounded_wait_probe_kernel(long long limit, int* err) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    const bool ok = mbar_wait(&bar, 0, &abort_flag, limit);
+    if (!ok) atomicExch(err, 1);
+    mbar_inval(&bar);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_bounded_wait_probe(Context& ctx, long long limit_cycles) {
+  int* err = reinterpret_cast<int*>(ctx.scratch(Context::kTensorAux, 256));
+  bounded_wait_probe_kernel<<<1, 32, 0, ctx.stream>>>(limit_cycles, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl, const DevImage& dst,
                      bool forced) {
   if (m == kAbsDistance) return false;

@@ -32,6 +32,11 @@ cudaError_t proximity_backward(Context& ctx, const DevImage& S, const DevImage& 
                                const DevImage* G1, const DevImage* G2, const DevImage* N2,
                                const DevImage* dS, const DevImage* dT);
 
+// Launches a kernel whose one thread waits on an mbarrier that nothing arrives
+// on, bounded to `limit_cycles` SM clock cycles (the failure path of every
+// wait in the tensor kernels, exercised without a fault).
+cudaError_t launch_bounded_wait_probe(Context& ctx, long long limit_cycles);
+
 // A prepared batch: every (image i, template j) pair into dsts[i * ntpl + j],
 // one persistent launch over a work queue of (pair, channel, strip, band)
 // items, captured in a CUDA graph. All images share one type; every pair must

@@ -101,6 +101,16 @@ def _load():
                                             ctypes.POINTER(vp)]),
         "ocipRunProximityBatch": (i32, [vp]),
         "ocipProximityBackward": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+        "ocipTestBoundedWait": (i32, [ctypes.c_int]),
+        "ocipPrepareStatistics": (i32, [ctypes.POINTER(vp), vp]),
+        "ocipMinIndx": (i32, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_int)]),
+        "ocipMaxIndx": (i32, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_int)]),
+        "ocipMinAbsIndx": (i32, [vp, vp, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+        "ocipMaxAbsIndx": (i32, [vp, vp, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "ocipGetProximityBatchInfo": (i32, [vp, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
@@ -337,6 +347,22 @@ def proximity_backward(S, T, G1=None, G2=None, N2=None, dS=None, dT=None):
     the error code."""
     h = lambda x: x.handle if x is not None else None
     return lib.ocipProximityBackward(h(S), h(T), h(G1), h(G2), h(N2), h(dS), h(dT))
+
+
+def prepare_statistics(img=None):
+    h = ctypes.c_void_p()
+    check(lib.ocipPrepareStatistics(ctypes.byref(h), img.handle if img else None),
+          "ocipPrepareStatistics")
+    return Program(h)
+
+
+def index_reduce(name, prog, img):
+    """ocip<name>(prog, img) for name in MinIndx, MaxIndx, MinAbsIndx, MaxAbsIndx:
+    (error code, value, x, y)."""
+    v, x, y = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    rc = getattr(lib, "ocip" + name)(prog.handle, img.handle, ctypes.byref(v), ctypes.byref(x),
+                                     ctypes.byref(y))
+    return rc, v.value, x.value, y.value
 
 
 def prepare_integral(img=None):

@@ -65,4 +65,11 @@ int orc_proximity_backward(int measure, const double* S, const double* T,
 #ifdef __cplusplus
 }
 #endif
+
+/* MinIndx (op 0), MaxIndx (1), MinAbsIndx (2), MaxAbsIndx (3) of a
+ * one-channel image, in the reference's comparison order
+ * (statistics_oracle.c). */
+int orc_index_reduce(int op, int type, const void* src, int step, int W, int H, double* value,
+                     int* x, int* y);
+
 #endif

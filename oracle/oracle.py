@@ -184,6 +184,23 @@ def window_terms_exact(src, tmpl):
     return e, x, t
 
 
+INDEX_OPS = {"MinIndx": 0, "MaxIndx": 1, "MinAbsIndx": 2, "MaxAbsIndx": 3}
+
+
+def index_reduce(name, src):
+    """(value, x, y) of ocip<name> on a one-channel image, in the
+    reference's comparison order."""
+    lib = _lib_orc()
+    src, sp, ss, w, h, c = _img(src)
+    assert c == 1
+    v, x, y = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    rc = lib.orc_index_reduce(INDEX_OPS[name], type_index(src), sp, ss, w, h, ctypes.byref(v),
+                              ctypes.byref(x), ctypes.byref(y))
+    if rc:
+        raise RuntimeError(f"oracle returned {rc}")
+    return v.value, x.value, y.value
+
+
 def integral_exact(src, sqr):
     lib = _lib_orc()
     src, sp, ss, w, h, c = _img(src)

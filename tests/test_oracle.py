@@ -161,3 +161,33 @@ def test_backward_oracle_matches_finite_differences():
             Sp[i, j] += h; Sm[i, j] -= h
             fd = (f(Sp, T) - f(Sm, T)) / (2 * h)
             assert abs(fd - dS[i, j]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_index_reduce_oracle_matches_brute_force_without_ties():
+    """With a unique extreme, the reference's reduction order does not matter:
+    the oracle's (value, x, y) equals numpy's argmin / argmax."""
+    rng = np.random.default_rng(21)
+    for shape in [(37, 300), (16, 256), (1, 1), (70, 513)]:
+        a = rng.permutation(shape[0] * shape[1]).reshape(shape).astype(np.float32) - 1000.0
+        for name, fn in [("MinIndx", np.argmin), ("MaxIndx", np.argmax),
+                         ("MinAbsIndx", lambda v: np.argmin(np.abs(v))),
+                         ("MaxAbsIndx", lambda v: np.argmax(np.abs(v)))]:
+            v, x, y = O.index_reduce(name, a)
+            iy, ix = np.unravel_index(fn(a), a.shape)
+            ref = a[iy, ix] if "Abs" not in name else abs(a[iy, ix])
+            assert (x, y) == (ix, iy) and v == ref, (name, shape)
+
+
+def test_index_reduce_oracle_tie_order():
+    """Ties follow the reference's reduction tree. Across 256 x 16 groups the
+    first group in row-major group order wins. Inside a group, a work-item
+    (lx, ly) keeps its first pixel of a tie along x, and the tree folds
+    lid + s into lid (s = 128 .. 1), an equal value never replacing: below,
+    row 9's candidate (lid 145) reaches lid 17 at the first level, before row
+    7's (lid 113, via lid 49 at s = 64) meets it at s = 32, so row 9 wins."""
+    a = np.zeros((40, 600), np.uint8) + 9
+    a[30, 5] = a[3, 100] = a[3, 516] = 1   # groups (x0, y1), (x0, y0), (x2, y0)
+    assert O.index_reduce("MinIndx", a) == (1.0, 100, 3)
+    b = np.zeros((16, 256), np.uint8) + 9
+    b[7, 33] = b[7, 17] = b[9, 1] = 1
+    assert O.index_reduce("MinIndx", b) == (1.0, 1, 9)

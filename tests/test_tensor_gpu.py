@@ -274,3 +274,20 @@ def test_cfg5_u16_full_size_accuracy_on_crops(ocip, ctx):
                 err = np.abs(sub - ex) / np.abs(ex)
             assert err.max() <= TOL, (MEAS[m], y, x, err.max())
     ctx.set_path(ocip.PATH_PLAIN)
+
+
+def test_bounded_wait_expires_and_context_stays_usable(ocip, ctx):
+    """A kernel waits on a barrier nothing arrives on: the bounded wait
+    expires (about 1 ms here), the kernel returns, the error surfaces as
+    CL_OUT_OF_RESOURCES at the next synchronisation, and the context keeps
+    working."""
+    ctx.make_current()
+    assert ocip.lib.ocipTestBoundedWait(2_000_000) == ocip.CL_OUT_OF_RESOURCES
+    assert ocip.lib.ocipFinish() == 0  # the flag was cleared
+    rng = np.random.default_rng(17)
+    S = rng.integers(0, 256, (64, 300), dtype=np.uint8)
+    T = rng.integers(0, 256, (9, 9), dtype=np.uint8)
+    got, path = run(ocip, ctx, 3, S, T, ocip.PATH_TENSOR)
+    assert path == ocip.PATH_TENSOR
+    assert np.array_equal(got, O.proximity_exact(3, S, T).astype(np.float32))
+    ctx.set_path(ocip.PATH_PLAIN)
