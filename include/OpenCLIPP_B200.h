@@ -136,7 +136,10 @@ ocipError ocip_API ocipProximityBackward(ocipImage Source, ocipImage Template,
  * bounded wait expired as designed. */
 ocipError ocip_API ocipTestBoundedWait(int LimitCycles);
 
-/* Device address and row pitch (bytes) of an image's device buffer. */
+/* Device address and row pitch (bytes) of an image's device buffer. Writes
+ * made through this address are not tracked by the library, so from then on
+ * ocipReadImage of this image waits for all work queued on the context's
+ * stream (otherwise a read waits only for the image's last writer). */
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,
                                          size_t* Pitch);
 

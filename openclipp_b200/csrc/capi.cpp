@@ -65,7 +65,20 @@ void send(Image& img) {
   check_cuda(cudaMemcpy2DAsync(img.dev, img.pitch, img.host, img.desc.Step, row,
                                img.desc.Height, cudaMemcpyHostToDevice, ctx.stream),
              "send image");
+  mark_written(img);
+}
+
+void mark_written(Image& img) {
   img.in_device = true;
+  if (img.written == nullptr)
+    check_cuda(cudaEventCreateWithFlags(&img.written, cudaEventDisableTiming), "event");
+  check_cuda(cudaEventRecord(img.written, img.ctx->stream), "event record");
+}
+
+void mark_untracked_writes(Context& ctx) {
+  if (ctx.untracked == nullptr)
+    check_cuda(cudaEventCreateWithFlags(&ctx.untracked, cudaEventDisableTiming), "event");
+  check_cuda(cudaEventRecord(ctx.untracked, ctx.stream), "event record");
 }
 
 void send_if_needed(Image& img) {
@@ -116,6 +129,8 @@ void Context::check_device_errors() {
 Context::~Context() {
   for (auto& s : scratch_)
     if (s.ptr) cudaFree(s.ptr);
+  if (untracked) cudaEventDestroy(untracked);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -155,6 +170,7 @@ ocipError ocipInitialize(ocipContext* ContextPtr, const char* PreferredPlatform,
     ctx->cc_major = prop.major;
     ctx->cc_minor = prop.minor;
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       delete ctx;
       check_cuda(e, "cudaStreamCreate");
@@ -263,11 +279,20 @@ ocipError ocipReadImage(ocipImage h) {
     if (img.host == nullptr) return CL_SUCCESS;  // Buffer.cpp:125-126
     Context& ctx = *img.ctx;
     check_cuda(cudaSetDevice(ctx.device), "cudaSetDevice");
+    // The copy waits for the image's last writer only, not for everything
+    // queued since: kernels enqueued after that writer keep running while
+    // this map travels to the host. The call still returns only once the
+    // data is in the host buffer (Read is blocking, OpenCLIPP.cpp:203-211),
+    // so no copy is ever left in flight across calls.
+    if (img.exposed) mark_written(img);  // writes through the raw address: wait for all
+    if (img.written) check_cuda(cudaStreamWaitEvent(ctx.copy_stream, img.written, 0), "read wait");
+    if (ctx.untracked)
+      check_cuda(cudaStreamWaitEvent(ctx.copy_stream, ctx.untracked, 0), "read wait");
     check_cuda(cudaMemcpy2DAsync(img.host, img.desc.Step, img.dev, img.pitch,
                                  img.row_bytes(), img.desc.Height,
-                                 cudaMemcpyDeviceToHost, ctx.stream),
+                                 cudaMemcpyDeviceToHost, ctx.copy_stream),
                "read image");
-    check_cuda(cudaStreamSynchronize(ctx.stream), "read image");
+    check_cuda(cudaStreamSynchronize(ctx.copy_stream), "read image");
     ctx.check_device_errors();
   )
 }
@@ -279,6 +304,7 @@ ocipError ocipReleaseImage(ocipImage h) {
       cudaSetDevice(img->ctx->device);
       cudaStreamSynchronize(img->ctx->stream);
     }
+    if (img->written) cudaEventDestroy(img->written);
     cudaFree(img->dev);
     img->magic = 0;
     delete img;
@@ -354,6 +380,7 @@ ocipError ocipGetImageDevicePtr(ocipImage h, void** DevicePtr, size_t* Pitch) {
     Image& img = image(h);
     if (DevicePtr) *DevicePtr = img.dev;
     if (Pitch) *Pitch = img.pitch;
+    img.exposed = true;
   )
 }
 

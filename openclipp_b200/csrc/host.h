@@ -31,6 +31,12 @@ struct Context {
   int sm_count = 0;
   int cc_major = 0, cc_minor = 0;
   cudaStream_t stream = nullptr;
+  // Device-to-host reads run here, after the event of the image's last
+  // writer, so a read of one score map overlaps kernels queued after it.
+  cudaStream_t copy_stream = nullptr;
+  // Recorded on `stream` after work whose destinations are not tracked per
+  // image (a replayed batch graph); every read also waits for it.
+  cudaEvent_t untracked = nullptr;
   std::string name;
   int path = 1;       // ocipProximityPath; PLAIN by default (the drop-in)
   int last_path = 1;  // path that served the last proximity call
@@ -62,6 +68,11 @@ struct Image {
   void* dev = nullptr;
   size_t pitch = 0;        // device row pitch, bytes (multiple of 128)
   bool in_device = false;  // Memory::m_isInDevice (C++/Buffer.cpp:30-43)
+  cudaEvent_t written = nullptr;  // recorded on the context's stream after the last write
+  // The device address was handed out (ocipGetImageDevicePtr): writes made
+  // through it are not tracked, so a read waits for all of the context's
+  // queued work.
+  bool exposed = false;
   size_t row_bytes() const {
     return (size_t)desc.Width * desc.Channels * type_bytes((int)desc.Type);
   }
@@ -102,6 +113,12 @@ Context& current();
 Image& image(ocipImage h);
 void send(Image& img);
 void send_if_needed(Image& img);
+// The image's device buffer has been written by work just queued on the
+// context's stream (a kernel or an upload): records its event.
+void mark_written(Image& img);
+// Work just queued on the context's stream wrote images that are not tracked
+// one by one: every later read waits for it.
+void mark_untracked_writes(Context& ctx);
 DevImage dev_view(const Image& img);
 
 }  // namespace ocipb

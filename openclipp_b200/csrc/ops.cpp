@@ -104,7 +104,7 @@ void proximity_run(Context& ctx, Measure m, Image& S, Image& T, Image& D, int pa
     ctx.last_path = OCIP_PATH_PLAIN;
   }
   check_cuda(e, "proximity kernel launch");
-  D.in_device = true;
+  mark_written(D);
 }
 
 void proximity(Measure m, ocipImage hs, ocipImage ht, ocipImage hd) {
@@ -194,7 +194,7 @@ void integral(bool sqr, ocipProgram hp, ocipImage hs, ocipImage hd) {
   check_cuda(launch_integral(sqr, dev_view(S), dev_view(D), prog.scratch, prog.scratch_bytes,
                              ctx.stream),
              "integral kernel launch");
-  D.in_device = true;
+  mark_written(D);
 }
 
 // Batched matching (extension, no reference counterpart): the checks of the
@@ -251,6 +251,7 @@ void batch_prepare(ocipProgram* out, int measure, const ocipImage* himgs, int ni
   p->ctx = &ctx;
   p->batch = b;
   for (Image* x : dsts) x->in_device = true;
+  mark_untracked_writes(ctx);  // the band-height tuning runs write destinations
   *out = reinterpret_cast<ocipProgram>(p);
 }
 
@@ -307,8 +308,8 @@ void backward(ocipImage hs, ocipImage ht, ocipImage hg1, ocipImage hg2, ocipImag
                                 G2 ? &vg2 : nullptr, N2 ? &vn2 : nullptr, dS ? &vds : nullptr,
                                 dT ? &vdt : nullptr),
              "backward launch");
-  if (dS) dS->in_device = true;
-  if (dT) dT->in_device = true;
+  if (dS) mark_written(*dS);
+  if (dT) mark_written(*dT);
 }
 
 // Statistics::Min/Max/MinAbs/MaxAbs with coordinates
@@ -396,6 +397,7 @@ ocipError ocipRunProximityBatch(ocipProgram P) {
     ocipb::Program& prog = program(P, ocipb::Program::kProximityBatch);
     if (prog.ctx != &ctx) fail(CL_INVALID_CONTEXT, "program belongs to another context");
     check_cuda(tensor_batch_run(prog.batch), "batch launch");
+    mark_untracked_writes(ctx);
   )
 }
 

@@ -200,3 +200,32 @@ def test_fft_named_entry_points(ocip, plain):
     assert ocip.lib.ocipCrossCorrFFT(prog.handle, Si.handle, T64.handle, Di.handle) == \
         ocip.CL_IMAGE_FORMAT_MISMATCH
     prog.release()
+
+
+def test_reads_overlap_later_kernels(ocip, ctx):
+    """Five maps queued, then read one by one: each read waits only for its own
+    writer (later kernels still run), and every map equals a lone call's."""
+    ctx.make_current()
+    ctx.set_path(ocip.PATH_AUTO)
+    try:
+        rng = np.random.default_rng(5)
+        S = rng.random((700, 900)).astype(np.float32)
+        T = S[100:131, 200:231].copy()
+        Si, Ti = ocip.Image(S), ocip.Image(T)
+        outs = [np.zeros(S.shape, np.float32) for _ in MEAS]
+        Ds = [ocip.Image(o) for o in outs]
+        for rep in range(2):
+            for o in outs:
+                o[:] = np.nan
+            for m, D in zip(MEAS, Ds):
+                ocip.check(ocip.proximity(m, Si, Ti, D), m)
+            for D in Ds:
+                D.read()
+            for m, o in zip(MEAS, outs):
+                assert np.array_equal(o, ocip.match(m, S, T), equal_nan=True), (rep, m)
+        for D in Ds:
+            D.release()
+        Si.release()
+        Ti.release()
+    finally:
+        ctx.set_path(ocip.PATH_PLAIN)
