@@ -35,6 +35,13 @@ ocipError ocip_API ocipGetProximityPath(int* Path);
  * (an ocipProximityPath value other than AUTO). */
 ocipError ocip_API ocipGetLastProximityPath(int* Path);
 
+/* Output rows per work item of the one-pair tensor-path launches of the
+ * current context (each item also reads the template's height less one rows
+ * above its band). 0, the default, picks the height per launch from the SM
+ * count and the number of column strips; a positive value (clamped to the
+ * image height) fixes it, for tuning and for tests. */
+ocipError ocip_API ocipSetProximityBandHeight(int Rows);
+
 /* Human-readable detail of the last error returned on this thread. */
 ocip_API const char* ocipGetLastErrorMessage(void);
 

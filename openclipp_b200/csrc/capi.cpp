@@ -358,6 +358,15 @@ ocipError ocipGetLastProximityPath(int* Path) {
   )
 }
 
+ocipError ocipSetProximityBandHeight(int Rows) {
+  if (g_current == nullptr) return CL_INVALID_CONTEXT;
+  OCIP_GUARD(
+    Context& ctx = current();
+    if (Rows < 0) fail(CL_INVALID_VALUE, "Rows is negative");
+    ctx.band_rows = Rows;
+  )
+}
+
 const char* ocipGetLastErrorMessage(void) { return g_last_error.c_str(); }
 
 ocipError ocipGetStream(void** Stream) {

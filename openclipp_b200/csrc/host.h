@@ -40,6 +40,7 @@ struct Context {
   std::string name;
   int path = 1;       // ocipProximityPath; PLAIN by default (the drop-in)
   int last_path = 1;  // path that served the last proximity call
+  int band_rows = 0;  // output rows per tensor work item; 0: chosen per launch
   void* scratch(int slot, size_t bytes);
   // The tensor-path kernels set a device flag (kTensorAux scratch) when a
   // bounded wait expires (the kernel then returns without finishing its

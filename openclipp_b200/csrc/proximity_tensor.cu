@@ -2,57 +2,71 @@
 //
 // The product term of SqrDistance[_Norm] and CrossCorr[_Norm]
 // (cl-files/ImageProximity.cl :44, :122, :290, :375),
-//   C(x, y) = sum_h sum_w S(x + w - tw/2, y + h - th/2) * T(w, h),
-// is computed per channel as one small GEMM per source row r and 256-position
-// strip. Each TMEM lane m holds two output positions, x0 + 2m (phase 0) and
-// x0 + 2m + 1 (phase 1), and the A row of lane m is the source-row window
-//   A_r[m][k] = S(x0 - tw/2 + 2m + k, r),   k < K = roundup(tw + 1),
-// so the two phases share A: phase p reads it one pixel later. The template
-// operand has N = 2R rows (R = th rounded up to 16/32/64, zero rows on top),
-//   B[p R + n][k] = Tpad(k - p, n),   Tpad(w, n) = T(w, n - (R - th)),
-// and D_r[m][p R + n] is the contribution of template row n to position
-// x0 + 2m + p. Source row r feeds output row y = r - n + off
-// (off = R - th + th/2) through template row n, so every output row collects
-// R consecutive steps. The epilogue keeps those R partial sums per position
-// in registers, ordered by output row: at each step it adds the step's R
-// columns and shifts by one (acc[c] <- acc[c + 1] + D[R - 2 - c]), and
-// acc[0] + D[R - 1] is the finished output row.
+//   C(x, y) = sum_h sum_w S(x + w - ax, y + h - ay) * T(w, h),
+// is computed per channel and strip of P = 128 S output positions by one
+// chain of MMAs per source row. TMEM lane m holds the S positions
+// x0 + S m + p (p < S). R (template rows rounded up to 16, 32 or 64) and S
+// satisfy S R = 128: S = 8, 4, 2. An MMA instruction (M = 128, K = 16) takes
+// the same time for any N up to 256, so the kernel makes N as wide as the
+// accumulators in TMEM allow.
 //
-// The A operand lives in tensor memory: builder warps write each lane's
-// K-pixel window with tcgen05.st (BF16 hi/lo pairs for F32 and U16 sources,
-// bytes for U8), and the MMA reads it from TMEM, which costs half as many
-// cycles per instruction as an A operand read from shared memory.
+// A operand (shared memory, no per-lane copies). Lane m's K window is the
+// staged row itself, A[m][k] = raw(S m + k): a Hankel matrix. In the
+// canonical K-major SWIZZLE_NONE layout a core matrix row is 16 bytes, so the
+// row is stored once more per S pixels: buffer row q holds raw elements
+// S q .. S q + 7 (BF16) or .. + 15 (i8), and core matrix c of lane m is buffer
+// row m + c (8/S) [(16/S) for i8]: one descriptor per MMA with SBO = 128 and
+// LBO = the distance of the next K core matrix.
 //
-// Channels. Interleaved multi-channel sources are first split into planes
-// (one row-major plane per channel in scratch memory); blockIdx.z is the
-// channel, the TMA view has the channel as its outermost dimension (so rows
-// outside a plane read as zeros), and the template and the score map are
-// addressed with the channel stride.
+// F32 and U16 sources are split into BF16 hi + lo (U16 exactly) and three
+// products hi*Thi + hi*Tlo + lo*Thi accumulate in FP32. They are packed into
+// MMAs of K = 16 by pairing core matrices along K: (hi_c, lo_c) x (Tlo_c, Thi_c)
+// for every chunk c, then (hi_2i, hi_2i+1) x (Thi_2i, Thi_2i+1). U8 sources use
+// the i8 MMA with s32 accumulation (exact).
 //
-// Precision. U8 sources use the i8 MMA with s32 accumulation: every product
-// term is exact and so are the results. F32 and U16 sources are split into
-// BF16 hi + lo parts (S = S_hi + S_lo + O(2^-18 S); exact for U16); three MMAs
-// (hi*hi, hi*lo, lo*hi) accumulate in FP32 in TMEM. The window energy sum S^2
-// of each position is a per-row sum of tw squares (FP32 FMA for F32, FP64 for
-// U16, exact integers for U8) and a running sum over the last th rows (FP64 /
-// exact integers); the template energy is exact in FP64. SqrDistance =
-// E_S - 2C + E_T and the _Norm scale are done in FP64 (F32, U16) or as the
-// plain path does them (U8).
+// B operand: N = S R = 128 rows, row S j + p = template row th - 1 - j at phase
+// p, shifted by the staged row's lead: B[S j + p][k] = T(k - p - lead, th-1-j).
+// Source row t then adds to output-row slots t .. t + R - 1 (slot u is the
+// output row whose last template row is source row u).
 //
-// Roles (17 warps; one CTA per SM, since it allocates all of TMEM):
-//   warps 0-7   builders, two per TMEM sub-partition (tcgen05.ld/st reach
-//               only the 32 lanes of the warp's sub-partition), one per phase:
-//               the A operand of step t (the warp's half of the K columns) and
-//               the window energy of its positions, handed to the epilogue
-//               through a shared-memory ring;
-//   warps 8-15  epilogue, same split: TMEM loads, running sums, output;
-//   warp 16     control: TMA loads of source rows (zero fill outside the
-//               image) and the MMAs of each step. Issuing an MMA or a commit
-//               blocks the issuing thread for tens of cycles, so this thread
-//               does nothing else: one wait (ready), the MMAs, one commit
-//               (mma_done) per step.
-// Stages are chained by mbarriers; every wait is bounded and sets an error
-// flag instead of hanging.
+// Blocks. The steps (source rows) of an item are cut into blocks of
+// B = 16 / S steps. Step q of a block adds into TMEM columns S q + [0, N) of
+// the block's partial buffer: MMAs of N' = N + 16 = 144 columns at the
+// buffer's first column with B read S q rows later (B is stored with 16 - S
+// zero rows in front), so the block's partial sums of its B + R - 1 slots
+// end up at columns S j + p. The block's first MMA does not accumulate, which
+// clears the buffer. Partial buffers are double-buffered: the epilogue reads
+// block k while the tensor cores fill block k + 1.
+//
+// Running sums. The epilogue adds each block's partials into a ring of
+// running sums in TMEM that only it reads and writes (slot u at ring columns
+// S (u mod NS) + p, NS S = 144 columns; FP32 round-to-nearest, exact int32
+// for U8). The block's first 16 columns are the B slots it completes: the
+// epilogue writes them out and clears their ring columns. The tensor cores'
+// FP32 accumulation into one value thus never spans more than one block:
+// that accumulator rounds every addition with a bias that grows with the
+// number of additions, so the chains of a whole window (th rows x K chunks)
+// would cost accuracy.
+//
+// Window energy sum S^2 of each position: per source row the energy warps sum
+// tw squares per position (FP32 FMA for F32, exact integers for U8 and U16;
+// the S positions of a thread are independent chains), keep the row sums in a
+// ring of R rows and a running sum over the last th rows (FP64 or exact
+// integers) and hand the window sums to the epilogue through a ring in shared
+// memory whose entries the epilogue releases. SqrDistance = E_S - 2C + E_T and the _Norm scale are
+// done in FP64 (F32, U16) or as the plain path does them (U8: the results are
+// bit-identical to it).
+//
+// Roles (14 warps; one CTA per SM, which holds all 512 TMEM columns):
+//   warps 0-3  builders: the A operand of each row (split into hi/lo);
+//   warps 4-7  epilogue (warp 4 + k reads TMEM lanes 32k .. 32k + 31): running
+//              sums in the TMEM ring, score map;
+//   warp 8     TMA loads of source rows (zero fill outside the image);
+//   warp 9     MMA issue (one commit per source row, one per block);
+//   warps 10-13 window energies (measures other than CrossCorr).
+// Every wait is bounded: a wait that gives up sets the CTA's abort flag, the
+// roles leave their loops, the MMA and TMA threads drain what they issued,
+// and the kernel raises the context's error flag.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -75,17 +89,27 @@ namespace {
 using namespace sm100;
 
 constexpr int kM = 128;                 // TMEM lanes = A rows
-constexpr int kPos = 2 * kM;            // output positions per strip
-constexpr int kBuilders = 8;
-constexpr int kEpilogue = 8;
-constexpr int kThreads = (kBuilders + kEpilogue + 1) * 32;  // + control warp
-constexpr int kRB = 8;                  // source rows per TMA load
-constexpr int kNRaw = 4;                // TMA stages
-constexpr int kNE = 16;                 // window-energy ring depth (steps)
+constexpr int kBuilders = 4;
+constexpr int kEpilogue = 4;
+constexpr int kTmaWarp = kBuilders + kEpilogue;
+constexpr int kMmaWarp = kTmaWarp + 1;
+constexpr int kEnergyWarp = kMmaWarp + 1;  // first of the window-energy warps
+constexpr int kEnergy = 4;
+constexpr int kThreads = (kEnergyWarp + kEnergy) * 32;
+constexpr int kBuildThreads = kBuilders * 32;
+constexpr int kNRaw = 6;                // staged source rows (TMA stages of one row)
+constexpr int kNA = 4;                  // A operand stages (one source row each)
+constexpr int kSR = 128;                // S R: template rows x positions per lane
+constexpr int kN = kSR;                 // B rows (MMA N without the slide)
+constexpr int kNp = kN + 16;            // MMA N: a block's B - 1 slides fit in 16 more
+constexpr int kPartCols = kNp;          // TMEM columns per partial buffer (two of them)
+constexpr int kRingCol = 2 * kPartCols; // first TMEM column of the running-sum ring
+constexpr int kRingCols = kNp;          // ring columns: NS S = 144 (9 chunks of 16)
 constexpr int kTmemCols = 512;
 constexpr int kMinSmem = 120 * 1024;    // keeps one CTA per SM (it takes all of TMEM)
 constexpr int kMaxDynSmem = 226 * 1024; // opt-in dynamic shared memory limit of the kernel
 constexpr long long kSpinLimit = 4000000000LL;  // about 2 s of SM clock
+constexpr int kBarBuild = 1;            // named barrier of the builder warps
 
 enum Elem { kF32 = 0, kU8 = 1, kU16 = 2 };
 
@@ -94,32 +118,81 @@ struct ElemTraits {
   static constexpr bool split = ELEM != kU8;  // BF16 hi/lo operands
   static constexpr int size = ELEM == kF32 ? 4 : ELEM == kU16 ? 2 : 1;
   static constexpr int inner = 16 / size;     // elements per 16-byte TMA group
-  typedef typename std::conditional<split, float, int>::type AT;   // accumulators
-  typedef typename std::conditional<split, double, int>::type ET;  // window energy
+  static constexpr int cmk = split ? 8 : 16;  // K elements per core-matrix row
+  // Row sums of squares: FP32 for F32 sources, exact integers otherwise.
+  typedef typename std::conditional<
+      ELEM == kF32, float, typename std::conditional<ELEM == kU16, unsigned long long,
+                                                     int>::type>::type RT;
+  // Running window sums: FP64 for F32, exact integers otherwise.
+  typedef typename std::conditional<
+      ELEM == kF32, double, typename std::conditional<ELEM == kU16, unsigned long long,
+                                                     int>::type>::type WT;
+  // Row sums kept in the ring, window sums handed to the epilogue.
+  typedef typename std::conditional<split, float, int>::type ST;
 };
 
-// TMEM stages: NS stages of D (2R columns) first, then NS stages of A.
-template <int ELEM, int R, int K>
-struct Stages {
-  static constexpr int N2 = 2 * R;
-  static constexpr int AC = ElemTraits<ELEM>::split ? K : K / 4;  // TMEM columns per A stage
-  static constexpr int NS0 = kTmemCols / (N2 + AC);
-  static constexpr int NS = NS0 > 4 ? 4 : NS0;
-  static_assert(NS >= 2, "TMEM too small for two stages");
-  static_assert(2 * NS <= kNE, "energy ring shorter than the pipeline");
+// Positions per TMEM lane for a template of R rows (S R = 128), and the steps
+// of a block (S B = 16: a block's completed slots are one 16-column chunk).
+__host__ __device__ constexpr int s_for(int R) { return kSR / R; }
+__host__ __device__ constexpr int block_steps(int S) { return 16 / S; }
+
+// Geometry of one work item (host and device).
+struct Geo {
+  int S, P, Q, R, B;
+  int NB;          // B-operand rows stored per core matrix
+  int KC;          // core matrices of one K segment
+  int nmma;        // MMAs per source row
+  int cma;         // A core matrices addressed per lane (hi, incl. the pairing's spare)
+  int QR;          // buffer rows of one A plane
+  int lbok;        // bytes between K-adjacent core matrices of A
+  int nraw;        // staged elements the energies read (lead + P - 1 + tw)
+  int kNE;         // depth of the window-energy ring (steps, at most 16)
 };
 
-// One work item: one channel of one 256-position strip x band of rows of one
+__host__ __device__ inline Geo make_geo(bool split, int R, int tw, int lead) {
+  Geo g;
+  g.S = s_for(R);
+  g.P = kM * g.S;
+  g.Q = 16 / g.S;
+  g.R = R;
+  g.B = block_steps(g.S);
+  g.NB = kN + 32 - g.S;
+  const int cmk = split ? 8 : 16;
+  const int keff = tw + g.S - 1 + lead;
+  g.KC = (keff + cmk - 1) / cmk;
+  if (split) {
+    g.nmma = g.KC + (g.KC + 1) / 2;
+    g.cma = 2 * ((g.KC + 1) / 2);
+  } else {
+    g.nmma = (g.KC + 1) / 2;
+    g.cma = 2 * g.nmma;
+  }
+  g.lbok = 16 * (cmk / g.S);
+  g.QR = kM + (cmk / g.S) * (g.cma - 1);
+  g.nraw = lead + g.P - 1 + tw;
+  // Depth of the window-energy ring (each entry is released by the epilogue).
+  g.kNE = g.S == 8 ? 8 : 16;
+  return g;
+}
+
+// Staged elements of one row: the last buffer row's end, and every element
+// the energies read.
+__host__ __device__ inline int staged_elems(const Geo& g, bool split) {
+  const int a = g.S * (g.QR - 1) + (split ? 8 : 16);
+  return a > g.nraw ? a : g.nraw;
+}
+
+// One work item: one channel of one strip x band of rows of one
 // (image, template) pair.
 struct ItemArgs {
   const CUtensorMap* tmap;  // source planes (rank 4: group, groups, rows, channel)
   int W, H;
-  int tw, th;
+  int tw, th, R;
   int ax, ay;    // window anchor: output (x, y) reads S(x + w - ax, y + h - ay)
   int nch, ch;
-  int xs_out;    // strip covers outputs [xs_out, xs_out + 256)
+  int xs_out;    // strip covers outputs [xs_out, xs_out + P)
   int y0, yend;  // band of output rows
-  int nbox;      // 16-byte groups per staged row (the tensor map's box)
+  int nbox;      // 16-byte groups per staged row (box_split loads of box_part)
   const char* tmpl;
   size_t tmpl_pitch;
   char* dst;
@@ -130,24 +203,34 @@ struct ItemArgs {
 
 // Shared-memory layout, identical on host and device.
 struct Layout {
-  int row_bytes, raw_stage, raw, b_arr, b, rs, es, bars, total;
+  int row_bytes, raw_stage, raw, b, a_stage, a, rs, es, bars, total;
 };
 
 __host__ __device__ inline int align128(int x) { return (x + 127) & ~127; }
 
-__host__ __device__ inline Layout make_layout(bool split, int R, int K, int nbox) {
+// A staged row of nbox 16-byte groups is loaded by box_split(nbox) TMA copies
+// of box_part(nbox) groups each: a box dimension holds at most 256, and every
+// copy's shared-memory destination must be 128-byte aligned, so a part is a
+// multiple of 8 groups.
+__host__ __device__ inline int box_split(int nbox) { return (nbox + 255) / 256; }
+__host__ __device__ inline int box_part(int nbox) {
+  return ((nbox + box_split(nbox) - 1) / box_split(nbox) + 7) & ~7;
+}
+
+__host__ __device__ inline Layout make_layout(bool split, const Geo& g, int nbox) {
   Layout L;
-  L.row_bytes = nbox * 16;
-  L.raw_stage = align128(kRB * L.row_bytes);
+  L.row_bytes = box_split(nbox) * box_part(nbox) * 16;
+  L.raw_stage = align128(L.row_bytes);
   L.raw = 0;
-  L.b_arr = 2 * R * K * (split ? 2 : 1);
   L.b = L.raw + kNRaw * L.raw_stage;
-  L.rs = L.b + align128((split ? 2 : 1) * L.b_arr);
-  L.es = L.rs + R * kPos * 4;
-  L.bars = L.es + kNE * kPos * (split ? 8 : 4);
-  // mbarriers: raw full; ready and MMA done (4 each at most); energy full;
-  // done.
-  L.total = L.bars + align128(8 * (kNRaw + 2 * 4 + kNE + 1));
+  L.a = L.b + align128(2 * g.nmma * g.NB * 16);
+  L.a_stage = align128(g.QR * 16 * (split ? 2 : 1));
+  L.rs = L.a + kNA * L.a_stage;
+  L.es = L.rs + g.R * g.P * 4;
+  L.bars = L.es + g.kNE * g.P * 4;
+  // raw full, raw free; ready, MMA done; energy full, energy free (16 each
+  // at most); block full, buffer free; done.
+  L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNA + 32 + 4 + 1));
   return L;
 }
 
@@ -176,124 +259,181 @@ __device__ __forceinline__ double tmpl_at(const ItemArgs& a, int h, int w, int c
   return reinterpret_cast<const uint8_t*>(row)[i];
 }
 
-// Pixels e0 + 16c .. e0 + 16c + 15 of a staged row as floats (F32, U16).
+// Square of staged element e of a row, in the row-sum type.
 template <int ELEM>
-__device__ __forceinline__ void load_chunk(const unsigned char* row, int e0, int c, float (&f)[16]) {
+__device__ __forceinline__ typename ElemTraits<ELEM>::RT sq_at(const unsigned char* row, int e) {
   if (ELEM == kF32) {
-    const float2* r2 = reinterpret_cast<const float2*>(row) + (e0 >> 1) + c * 8;
-    if (e0 & 1) {  // odd start: aligned pairs from e0 - 1, shifted by one
-      float prev = r2[0].y;
+    const float v = reinterpret_cast<const float*>(row)[e];
+    return v * v;
+  }
+  if (ELEM == kU16) {
+    const unsigned int v = reinterpret_cast<const uint16_t*>(row)[e];
+    return static_cast<unsigned long long>(v * v);
+  }
+  const int v = reinterpret_cast<const uint8_t*>(row)[e];
+  return v * v;
+}
+
+// 8 staged elements from element e0 as floats (F32, U16).
+template <int ELEM, int S>
+__device__ __forceinline__ void load8(const unsigned char* row, int e0, float (&f)[8]) {
+  if (S == 1) {
+    // Any start element: single-element loads.
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float2 v = r2[j + 1];
-        f[2 * j] = prev;
-        f[2 * j + 1] = v.x;
-        prev = v.y;
-      }
+    for (int j = 0; j < 8; ++j) {
+      if (ELEM == kF32)
+        f[j] = reinterpret_cast<const float*>(row)[e0 + j];
+      else
+        f[j] = static_cast<float>(reinterpret_cast<const uint16_t*>(row)[e0 + j]);
+    }
+  } else if (ELEM == kF32) {
+    if (S % 4 == 0) {
+      const float4* p = reinterpret_cast<const float4*>(row + 4 * e0);
+      const float4 u = p[0], v = p[1];
+      f[0] = u.x; f[1] = u.y; f[2] = u.z; f[3] = u.w;
+      f[4] = v.x; f[5] = v.y; f[6] = v.z; f[7] = v.w;
     } else {
+      const float2* p = reinterpret_cast<const float2*>(row + 4 * e0);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float2 v = r2[j];
-        f[2 * j] = v.x;
-        f[2 * j + 1] = v.y;
+      for (int j = 0; j < 4; ++j) {
+        const float2 u = p[j];
+        f[2 * j] = u.x;
+        f[2 * j + 1] = u.y;
       }
     }
   } else {
-    // U16: 32-bit words hold two pixels; an odd start is realigned by bytes.
-    const uint32_t* r32 = reinterpret_cast<const uint32_t*>(row) + (e0 >> 1) + c * 8;
-    uint32_t w[9];
+    // U16: e0 is even (S = 2, 4 or 8), so 32-bit words hold pixel pairs.
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(row + 2 * e0);
 #pragma unroll
-    for (int j = 0; j < 9; ++j) w[j] = r32[j];
-    const bool odd = e0 & 1;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint32_t v = odd ? __byte_perm(w[j], w[j + 1], 0x5432) : w[j];
-      f[2 * j] = static_cast<float>(v & 0xFFFFu);
-      f[2 * j + 1] = static_cast<float>(v >> 16);
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t w = p[j];
+      f[2 * j] = static_cast<float>(w & 0xFFFFu);
+      f[2 * j + 1] = static_cast<float>(w >> 16);
     }
   }
 }
 
-// Runs one work item with all 17 warps of the CTA. The caller has synchronised
-// the CTA; TMEM (512 columns) is allocated. Barriers are initialised here and
-// invalidated at the end, so consecutive items may use different layouts.
-template <int ELEM, int R, int K>
+// AND of `p` over the builder warps (a named barrier every builder reaches).
+__device__ __forceinline__ bool builders_all(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "barrier.red.and.pred po, %2, %3, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)p), "n"(kBarBuild), "n"(kBuildThreads)
+      : "memory");
+  return r != 0;
+}
+
+// Runs one work item with all 14 warps of the CTA. The caller has
+// synchronised the CTA; TMEM (512 columns) is allocated. Barriers are
+// initialised here and invalidated at the end, so consecutive items may use
+// different layouts.
+template <int ELEM, int S>
 __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem, CtaState& cs) {
   typedef ElemTraits<ELEM> TR;
   constexpr bool SPLIT = TR::split;
-  typedef Stages<ELEM, R, K> SG;
-  constexpr int N2 = SG::N2, AC = SG::AC, NS = SG::NS;
-  typedef typename TR::AT AT;
-  typedef typename TR::ET ET;
-  typedef typename std::conditional<ELEM == kF32, float, ET>::type RT;  // row energy sum
-  // Row energies kept for th steps: FP32 for F32/U16 (the same rounded value
-  // is added and later subtracted, so the FP64 running sum does not drift),
-  // exact int for U8.
-  typedef typename std::conditional<SPLIT, float, int>::type ST;
-  const Layout L = make_layout(SPLIT, R, K, a.nbox);
+  constexpr int R = kSR / S;
+  constexpr int P = kM * S;
+  constexpr int Q = 16 / S;
+  constexpr int BS = block_steps(S);
+  constexpr int CMK = TR::cmk;
+  constexpr int NC = S * (BS + R - 1);  // open-slot columns of a block
+  constexpr int NCH = (NC + 15) / 16;   // 16-column chunks of a partial
+  static_assert(S * BS == 16, "a block's completed slots are one chunk");
+  static_assert(NC <= kNp && NCH * 16 == kRingCols, "block does not fit the ring");
+  typedef typename TR::RT RT;
+  typedef typename TR::WT WT;
+  typedef typename TR::ST ST;
+  const int lead = (TR::inner - a.ax % TR::inner) % TR::inner;
+  const Geo G = make_geo(SPLIT, R, a.tw, lead);
+  const Layout L = make_layout(SPLIT, G, a.nbox);
+  const int kNE = G.kNE;
 
-  // ready[i]: step t = i + k NS may be issued (its A operand is written and
-  //           the D stage of step t - NS has been read); 8 builder + 8
-  //           epilogue arrivals.
-  // mma_done[i]: the MMAs of step t have completed (D readable, A reusable).
   uint64_t* raw_full = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* ready = raw_full + kNRaw;
-  uint64_t* mma_done = ready + 4;
-  uint64_t* e_full = mma_done + 4;
-  uint64_t* done_bar = e_full + kNE;
+  uint64_t* raw_free = raw_full + kNRaw;
+  uint64_t* ready = raw_free + kNRaw;      // A of row t written
+  uint64_t* mma_done = ready + kNA;        // MMAs of row t complete (A stage free)
+  uint64_t* e_full = mma_done + kNA;       // window energies of row t written
+  uint64_t* e_free = e_full + 16;          // ... read by the epilogue
+  uint64_t* blk_full = e_free + 16;        // block's MMAs complete (2 buffers)
+  uint64_t* buf_free = blk_full + 2;       // block's buffer read by the epilogue
+  uint64_t* done_bar = buf_free + 2;
   volatile int* abort_flag = &cs.abort;
-  ET* estage = reinterpret_cast<ET*>(smem + L.es);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const bool need_e = a.measure != kCrossCorr;
   const int ch = a.ch;
-  const int left0 = a.ax;
-  // Staged rows start `lead` pixels before the strip's first window pixel,
-  // at a whole 16-byte group (TMA alignment).
-  const int lead = (TR::inner - left0 % TR::inner) % TR::inner;
-  const int off = R - a.th + a.ay;
-  const int r_begin = a.y0 - off;
+  const int r_begin = a.y0 - a.ay - (R - a.th);
   const int nsteps = (a.yend - a.y0) + R - 1;
-  const int nb = (nsteps + kRB - 1) / kRB;  // TMA loads (kRB rows each)
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kNRaw; ++i) mbar_init(&raw_full[i], 1);
-    for (int i = 0; i < NS; ++i) {
-      mbar_init(&ready[i], kBuilders + kEpilogue);
+    for (int i = 0; i < kNRaw; ++i) {
+      mbar_init(&raw_full[i], 1);
+      mbar_init(&raw_free[i], kBuilders + (need_e ? kEnergy : 0));
+    }
+    for (int i = 0; i < kNA; ++i) {
+      mbar_init(&ready[i], kBuilders);
       mbar_init(&mma_done[i], 1);
     }
-    for (int i = 0; i < kNE; ++i) mbar_init(&e_full[i], kBuilders);
+    for (int i = 0; i < kNE; ++i) {
+      mbar_init(&e_full[i], kEnergy);
+      mbar_init(&e_free[i], kEpilogue);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&blk_full[i], 1);
+      mbar_init(&buf_free[i], kEpilogue);
+    }
     mbar_init(done_bar, 1);
     fence_barrier_init();
-    // The first NS steps have no earlier D stage to wait for.
-    for (int i = 0; i < NS; ++i) mbar_arrive_n(&ready[i], kEpilogue);
   }
 
-  // Template operand B (N2 = 2R rows: phase 0 then phase 1, zero rows on top
-  // of each) and the template energy of this channel.
+  // Template operand B: per core matrix (two per MMA, in issue order) NB rows
+  // of 16 bytes; rows 16 - S .. 16 - S + N - 1 hold B, the rest are zero.
   {
-    const int padrows = R - a.th;
-    for (int idx = threadIdx.x; idx < N2 * K; idx += kThreads) {
-      const int nn = idx / K, k = idx - nn * K;
-      const int ph = nn >= R ? 1 : 0;
-      const int h = nn - ph * R - padrows;
-      const int w = k - ph;
-      const bool in = h >= 0 && w >= 0 && w < a.tw;
-      const double t = in ? tmpl_at<ELEM>(a, h, w, ch) : 0.0;
+    const int zp = 16 - S;
+    const int total = 2 * G.nmma * G.NB * CMK;
+    for (int idx = threadIdx.x; idx < total; idx += kThreads) {
+      const int e = idx % CMK;
+      const int row = (idx / CMK) % G.NB;
+      const int cm = idx / (CMK * G.NB);
+      // Which part (0 zero, 1 Thi, 2 Tlo; U8: 1) and which K chunk.
+      int part, c;
+      if (SPLIT) {
+        const int j = cm >> 1, half = cm & 1;
+        if (j < G.KC) {
+          c = j;
+          part = half ? 1 : 2;  // (hi_c, lo_c) x (Tlo_c, Thi_c)
+        } else {
+          c = 2 * (j - G.KC) + half;
+          part = c < G.KC ? 1 : 0;
+        }
+      } else {
+        c = cm;
+        part = c < G.KC ? 1 : 0;
+      }
+      const int n = row - zp;
+      double t = 0.0;
+      if (part && n >= 0 && n < kN) {
+        const int j = n / S, p = n - (n / S) * S;
+        const int h = a.th - 1 - j;
+        const int w = c * CMK + e - p - lead;
+        if (h >= 0 && w >= 0 && w < a.tw) t = tmpl_at<ELEM>(a, h, w, ch);
+      }
+      unsigned char* dst = smem + L.b + (cm * G.NB + row) * 16;
       if (SPLIT) {
         const float tf = static_cast<float>(t);
-        const __nv_bfloat16 th_ = __float2bfloat16_rn(tf);
-        const __nv_bfloat16 tl_ = __float2bfloat16_rn(tf - __bfloat162float(th_));
-        const int boff = ((k >> 3) * N2 + nn) * 16 + (k & 7) * 2;
-        *reinterpret_cast<__nv_bfloat16*>(smem + L.b + boff) = th_;
-        *reinterpret_cast<__nv_bfloat16*>(smem + L.b + L.b_arr + boff) = tl_;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(tf);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(tf - __bfloat162float(hi));
+        reinterpret_cast<__nv_bfloat16*>(dst)[e] = part == 2 ? lo : hi;
       } else {
-        const int boff = ((k >> 4) * N2 + nn) * 16 + (k & 15);
-        smem[L.b + boff] = static_cast<uint8_t>(t);
+        dst[e] = static_cast<uint8_t>(t);
       }
     }
-    if (warp == 1) {
+    if (warp == kTmaWarp) {
       double e = 0.0;
       for (int idx = lane; idx < a.th * a.tw; idx += 32) {
         const int h = idx / a.tw, k = idx - h * a.tw;
@@ -310,268 +450,325 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = cs.tmem;
-  constexpr uint32_t acol0 = NS * N2;  // first A column
 
-  const int sp = warp & 3;  // TMEM sub-partition of this warp
-  const int m = sp * 32 + lane;
-  const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(sp * 32) << 16);
-
-  if (warp == kBuilders + kEpilogue) {
-    // ---- Control: TMA loads of source rows, MMA issue ---------------------------
+  if (warp == kTmaWarp) {
+    // ---- TMA: source rows, one per stage ----------------------------------------
     if (lane == 0) {
       tma_prefetch_desc(a.tmap);
-      const int gx = (a.xs_out - left0 - lead) / TR::inner;
+      const int gx = (a.xs_out - a.ax - lead) / TR::inner;  // exact: a multiple of inner
+      const int part = box_part(a.nbox), nsplit = box_split(a.nbox);
       int issued = 0;
-      for (; issued < min(nb, kNRaw); ++issued) {
-        mbar_arrive_expect_tx(&raw_full[issued], kRB * L.row_bytes);
-        tma_load_4d(smem + L.raw + issued * L.raw_stage, a.tmap, 0, gx, r_begin + issued * kRB,
-                    ch, &raw_full[issued]);
+      for (; issued < nsteps; ++issued) {
+        const int st = issued % kNRaw;
+        if (issued >= kNRaw &&
+            !mbar_wait(&raw_free[st], ((issued / kNRaw) - 1) & 1, abort_flag, kSpinLimit))
+          break;
+        mbar_arrive_expect_tx(&raw_full[st], L.row_bytes);
+        for (int j = 0; j < nsplit; ++j)
+          tma_load_4d(smem + L.raw + st * L.raw_stage + j * part * 16, a.tmap, 0, gx + j * part,
+                      r_begin + issued, ch, &raw_full[st]);
       }
-      const uint32_t b0 = smem_u32(smem + L.b);
-      int i = 0, st = 0, rr = 0;
-      uint32_t ph = 0;
-      for (int t = 0; t < nsteps; ++t) {
-        if (!mbar_wait(&ready[i], ph, abort_flag, kSpinLimit)) break;
-        // Every builder has read row t: its stage is free after the last row.
-        if (rr == kRB - 1 && issued < nb) {
-          mbar_arrive_expect_tx(&raw_full[st], kRB * L.row_bytes);
-          tma_load_4d(smem + L.raw + st * L.raw_stage, a.tmap, 0, gx, r_begin + issued * kRB,
-                      ch, &raw_full[st]);
-          ++issued;
-        }
-        tc_fence_after();
-        const uint32_t d = tmem_base + i * N2;
-        const uint32_t at = tmem_base + acol0 + i * AC;
-        if (SPLIT) {
-          constexpr uint32_t idesc = idesc_bf16_f32(kM, N2);
-          const uint32_t blo = b0 + L.b_arr;
-#pragma unroll
-          for (int kk = 0; kk < K / 16; ++kk)
-            mma_bf16_ts(d, at + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
-                        kk > 0);
-#pragma unroll
-          for (int kk = 0; kk < K / 16; ++kk)
-            mma_bf16_ts(d, at + kk * 8, smem_desc(blo + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
-                        1);
-#pragma unroll
-          for (int kk = 0; kk < K / 16; ++kk)
-            mma_bf16_ts(d, at + K / 2 + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128),
-                        idesc, 1);
-        } else {
-          constexpr uint32_t idesc = idesc_u8_s32(kM, N2);
-#pragma unroll
-          for (int kk = 0; kk < K / 32; ++kk)
-            mma_i8_ts(d, at + kk * 8, smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128), idesc,
-                      kk > 0);
-        }
-        mma_commit(&mma_done[i]);
-        if (++i == NS) { i = 0; ph ^= 1; }
-        if (++rr == kRB) { rr = 0; if (++st == kNRaw) st = 0; }
-      }
-      // Every MMA issued has completed before the item ends (TMEM and the
-      // operands are reused), and every TMA load issued has landed.
-      mma_commit(done_bar);
+      // Every load issued has landed before the item ends.
       volatile int no_abort = 0;
-      mbar_wait(done_bar, 0, &no_abort, kSpinLimit);
       for (int b = max(0, issued - kNRaw); b < issued; ++b)
         mbar_wait(&raw_full[b % kNRaw], (b / kNRaw) & 1, &no_abort, kSpinLimit);
     }
+  } else if (warp == kMmaWarp) {
+    // ---- MMA issue --------------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = SPLIT ? idesc_bf16_f32(kM, kNp) : idesc_u8_s32(kM, kNp);
+      const uint32_t a0 = smem_u32(smem + L.a);
+      const uint32_t b0 = smem_u32(smem + L.b);
+      const uint32_t bstride = G.NB * 16;  // between B core matrices
+      int i = 0;
+      uint32_t ph = 0;
+      for (int t = 0; t < nsteps; ++t) {
+        const int k = t / BS, q = t - (t / BS) * BS;
+        // The buffer of block k was read by the epilogue (block k - 2).
+        if (q == 0 && k >= 2 &&
+            !mbar_wait(&buf_free[k & 1], ((k >> 1) - 1) & 1, abort_flag, kSpinLimit))
+          break;
+        if (!mbar_wait(&ready[i], ph, abort_flag, kSpinLimit)) break;
+        tc_fence_after();
+        const uint32_t d = tmem_base + (k & 1) * kPartCols;  // the block's partial
+        const uint32_t ah = a0 + i * L.a_stage;
+        const uint32_t bq = b0 + 16 * S * (Q - 1 - q);
+        // The block's first MMA overwrites all kNp columns of the partial.
+        const uint32_t acc0 = q == 0 ? 0u : 1u;
+        if (SPLIT) {
+          const uint32_t lo_off = G.QR * 16;
+          for (int c = 0; c < G.KC; ++c)
+            mma_bf16(d, smem_desc(ah + c * G.lbok, lo_off, 128),
+                     smem_desc(bq + 2 * c * bstride, bstride, 128), idesc, c == 0 ? acc0 : 1u);
+          for (int j = 0; j < G.nmma - G.KC; ++j)
+            mma_bf16(d, smem_desc(ah + 2 * j * G.lbok, G.lbok, 128),
+                     smem_desc(bq + 2 * (G.KC + j) * bstride, bstride, 128), idesc, 1u);
+        } else {
+          for (int j = 0; j < G.nmma; ++j)
+            mma_i8(d, smem_desc(ah + 2 * j * G.lbok, G.lbok, 128),
+                   smem_desc(bq + 2 * j * bstride, bstride, 128), idesc, j == 0 ? acc0 : 1u);
+        }
+        mma_commit(&mma_done[i]);
+        if (q == BS - 1 || t == nsteps - 1) mma_commit(&blk_full[k & 1]);
+        if (++i == kNA) { i = 0; ph ^= 1; }
+      }
+      // Every MMA issued has completed before the item ends.
+      mma_commit(done_bar);
+      volatile int no_abort = 0;
+      mbar_wait(done_bar, 0, &no_abort, kSpinLimit);
+    }
   } else if (warp < kBuilders) {
-    // ---- Builders: A operand of step t and the window energies ------------------
-    const int ph = warp >> 2;      // phase of the energies; K half of the A build
-    const int pos = 2 * m + ph;
-    const int e0 = lead + 2 * m;   // this lane's window starts at pixel e0 of the staged row
-    ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
-    ET ewin = ET(0);
-    int i = 0, st = 0, rr = 0;
+    // ---- Builders: A operand ------------------------------------------------------
+    const int b = threadIdx.x;  // 0 .. 127
+    int i = 0, st = 0;
     uint32_t iph = 0, rph = 0;
     for (int t = 0; t < nsteps; ++t) {
-      if (rr == 0 && !mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit)) break;
-      // A stage i is free once the MMAs of step t - NS have completed.
-      if (!mbar_wait(&mma_done[i], iph ^ 1, abort_flag, kSpinLimit)) break;
-      tc_fence_after();
-      const unsigned char* row = smem + L.raw + st * L.raw_stage + rr * L.row_bytes;
-      const uint32_t a_addr = lane_base + acol0 + i * AC;
-      ET rs = ET(0);
-      if (SPLIT) {
-        // The window in chunks of 16 K columns. The chunks alternate between
-        // the two builders of a lane; both read every chunk when energies are
-        // needed.
-        RT r0 = RT(0), r1 = RT(0);
+      bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
+      // A stage i is free once the MMAs of row t - kNA have completed.
+      ok = ok && (t < kNA || mbar_wait(&mma_done[i], iph ^ 1, abort_flag, kSpinLimit));
+      // All builders take the same branch (they meet at named barriers).
+      if (!builders_all(ok)) break;
+      const unsigned char* row = smem + L.raw + st * L.raw_stage;
+      unsigned char* ahi = smem + L.a + i * L.a_stage;
+      for (int q = b; q < G.QR; q += kBuildThreads) {
+        if (SPLIT) {
+          float f[8];
+          load8<ELEM, S>(row, S * q, f);
+          uint32_t hi[4], lo[4];
 #pragma unroll
-        for (int c = 0; c < K / 16; ++c) {
-          const bool mine = (c & 1) == ph;
-          if (!mine && !need_e) continue;
-          float f[16];
-          load_chunk<ELEM>(row, e0, c, f);
-          if (mine) {
-            uint32_t hi[8], lo[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              hi[q] = pack_bf16(f[2 * q], f[2 * q + 1]);
-              lo[q] = pack_bf16(f[2 * q] - bf16lo_f(hi[q]), f[2 * q + 1] - bf16hi_f(hi[q]));
-            }
-            tmem_st8(a_addr + c * 8, hi);
-            tmem_st8(a_addr + K / 2 + c * 8, lo);
+          for (int j = 0; j < 4; ++j) {
+            hi[j] = pack_bf16(f[2 * j], f[2 * j + 1]);
+            lo[j] = pack_bf16(f[2 * j] - bf16lo_f(hi[j]), f[2 * j + 1] - bf16hi_f(hi[j]));
           }
-          if (need_e) {
-            // Sum of squares over k in [ph, ph + tw). K = roundup16(tw + 1),
-            // so only k = 0 and the last chunk can fall outside.
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int k = c * 16 + j;
-              RT v = static_cast<RT>(f[j]);
-              if (k == 0 || k >= K - 16) v = (k >= ph && k < ph + a.tw) ? v : RT(0);
-              if (j & 1)
-                r1 = fma(v, v, r1);
-              else
-                r0 = fma(v, v, r0);
-            }
-          }
-        }
-        rs = static_cast<ET>(r0) + static_cast<ET>(r1);
-      } else {
-        // Bytes e0 .. e0 + K - 1 in chunks of 16 (4 TMEM columns): words
-        // from the aligned base, shifted. Chunks alternate between the two
-        // builders of a lane; both read every chunk when energies are needed.
-        const uint32_t* r32 = reinterpret_cast<const uint32_t*>(row) + (e0 >> 2);
-        const uint32_t sh = (e0 & 3) * 8;
-        const uint32_t sh2 = sh + 8 * ph;  // window of this builder's phase
-        uint32_t acc = 0;
-#pragma unroll
-        for (int c = 0; c < K / 16; ++c) {
-          const bool mine = (c & 1) == ph;
-          if (!mine && !need_e) continue;
+          *reinterpret_cast<uint4*>(ahi + q * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *reinterpret_cast<uint4*>(ahi + G.QR * 16 + q * 16) =
+              make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        } else {
+          // Bytes S q .. S q + 15 (S q is a multiple of 4 when S is).
+          const int off = S * q;
+          const uint32_t* w32 = reinterpret_cast<const uint32_t*>(row + (off & ~3));
+          const uint32_t sh = (off & 3) * 8;
           uint32_t w[5];
 #pragma unroll
-          for (int j = 0; j < 5; ++j) w[j] = r32[c * 4 + j];
-          if (mine) {
-            uint32_t av[4];
+          for (int j = 0; j < 5; ++j) w[j] = (S % 4 == 0 && j == 4) ? 0u : w32[j];
+          uint32_t v[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) av[j] = __funnelshift_r(w[j], w[j + 1], sh);
-            tmem_st4(a_addr + c * 4, av);
+          for (int j = 0; j < 4; ++j)
+            v[j] = S % 4 == 0 ? w[j] : __funnelshift_r(w[j], w[j + 1], sh);
+          *reinterpret_cast<uint4*>(ahi + q * 16) = make_uint4(v[0], v[1], v[2], v[3]);
+        }
+      }
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&ready[i]);
+        mbar_arrive(&raw_free[st]);
+      }
+      if (++i == kNA) { i = 0; iph ^= 1; }
+      if (++st == kNRaw) { st = 0; rph ^= 1; }
+    }
+  } else if (warp >= kEnergyWarp) {
+    // ---- Window energies ----------------------------------------------------------
+    // Positions x = b + 128 p: row sum of tw squares from staged element
+    // lead + x (the S positions of a thread are independent chains); the window
+    // sum adds this row and drops the row th steps back (the ring holds
+    // R >= th rows; read before write when th == R).
+    if (need_e) {
+      const int b = threadIdx.x - kEnergyWarp * 32;  // 0 .. 127
+      ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
+      ST* estage = reinterpret_cast<ST*>(smem + L.es);
+      WT ewin[S];
+#pragma unroll
+      for (int p = 0; p < S; ++p) ewin[p] = WT(0);
+      int st = 0;
+      uint32_t rph = 0;
+      for (int t = 0; t < nsteps; ++t) {
+        const int ei = t % kNE;
+        bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
+        // Ring entry ei was read by the epilogue (step t - kNE).
+        ok = ok && (t < kNE || mbar_wait(&e_free[ei], ((t / kNE) - 1) & 1, abort_flag, kSpinLimit));
+        if (!__all_sync(0xffffffffu, ok)) break;
+        const unsigned char* row = smem + L.raw + st * L.raw_stage;
+        ST* es = estage + ei * P;
+        RT rs[S];
+#pragma unroll
+        for (int p = 0; p < S; ++p) rs[p] = RT(0);
+        const int e0 = lead + b;
+        int w = 0;
+        for (; w + 4 <= a.tw; w += 4) {
+#pragma unroll
+          for (int d = 0; d < 4; ++d)
+#pragma unroll
+            for (int p = 0; p < S; ++p) rs[p] += sq_at<ELEM>(row, e0 + kBuildThreads * p + w + d);
+        }
+        for (; w < a.tw; ++w) {
+#pragma unroll
+          for (int p = 0; p < S; ++p) rs[p] += sq_at<ELEM>(row, e0 + kBuildThreads * p + w);
+        }
+#pragma unroll
+        for (int p = 0; p < S; ++p) {
+          const int x = b + kBuildThreads * p;
+          ST* slot = rsring + (t & (R - 1)) * P + x;
+          const ST old = t >= a.th ? rsring[((t - a.th) & (R - 1)) * P + x] : ST(0);
+          const ST cur = static_cast<ST>(rs[p]);
+          *slot = cur;
+          ewin[p] += static_cast<WT>(cur) - static_cast<WT>(old);
+          es[x] = static_cast<ST>(ewin[p]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&e_full[ei]);
+          mbar_arrive(&raw_free[st]);
+        }
+        if (++st == kNRaw) { st = 0; rph ^= 1; }
+      }
+    }
+  } else {
+    // ---- Epilogue ---------------------------------------------------------------
+    typedef typename std::conditional<SPLIT, float, int>::type AT;  // running sums
+    const int sp = warp - kBuilders;  // TMEM sub-partition (warp % 4)
+    const int m = sp * 32 + lane;
+    const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(sp * 32) << 16);
+    const uint32_t ring = lane_base + kRingCol;
+    const ST* estage = reinterpret_cast<const ST*>(smem + L.es);
+    const double etd = cs.et;
+    uint32_t zero[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) zero[j] = 0u;
+    for (int c = 0; c < kRingCols; c += 16) tmem_st16(ring + c, zero);
+    tmem_st_wait();
+    for (int k = 0; k * BS < nsteps; ++k) {
+      const int t0 = k * BS;
+      bool ok = mbar_wait(&blk_full[k & 1], (k >> 1) & 1, abort_flag, kSpinLimit);
+      // tcgen05.ld/st are warp-collective: the whole warp takes one branch.
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      const uint32_t part = lane_base + (k & 1) * kPartCols;
+      // Relative chunk i of the block lives at ring chunk (k + i) mod NCH.
+      // Chunks 1 .. NCH - 1 hold open slots: ring += partial.
+      for (int c16 = 1; c16 < NCH; ++c16) {
+        const uint32_t rc = ring + 16 * ((k + c16) % NCH);
+        uint32_t vp[16], vr[16];
+        tmem_ld16x(part + 16 * c16, vp);
+        tmem_ld16x(rc, vr);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          if (SPLIT)
+            vr[j] = __float_as_uint(__fadd_rn(__uint_as_float(vr[j]), __uint_as_float(vp[j])));
+          else
+            vr[j] += vp[j];  // exact int32 sums
+        }
+        tmem_st16(rc, vr);
+      }
+      // Chunk 0: the BS slots t0 .. t0 + BS - 1 this block completes. Their
+      // ring columns are cleared for the slots NS later.
+      AT val[16];
+      {
+        const uint32_t rc = ring + 16 * (k % NCH);
+        uint32_t vp[16], vr[16];
+        tmem_ld16x(part, vp);
+        tmem_ld16x(rc, vr);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          if (SPLIT)
+            val[j] = __fadd_rn(__uint_as_float(vr[j]), __uint_as_float(vp[j]));
+          else
+            val[j] = static_cast<int>(vr[j] + vp[j]);
+        }
+        tmem_st16(rc, zero);
+      }
+      tmem_st_wait();
+#pragma unroll
+      for (int g = 0; g < BS; ++g) {
+        const int u = t0 + g;
+        const int yd = a.y0 + u - R + 1;
+        if (u >= nsteps) break;
+        // Every step's energy entry is waited for and released in order, so
+        // the ring's barriers never run two phases apart.
+        ST e[S];
+        if (need_e) {
+          ok = mbar_wait(&e_full[u % kNE], (u / kNE) & 1, abort_flag, kSpinLimit);
+          if (!__all_sync(0xffffffffu, ok)) break;
+          const ST* ep = estage + (u % kNE) * P + S * m;
+#pragma unroll
+          for (int p = 0; p < S; ++p) e[p] = ep[p];
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&e_free[u % kNE]);
+        }
+        if (u >= R - 1 && yd < a.yend) {
+          char* orow = a.dst + (size_t)yd * a.dst_pitch;
+          float outf[S];
+          double outd[S];
+#pragma unroll
+          for (int p = 0; p < S; ++p) {
+            const AT cv = val[g * S + p];
+            if (SPLIT) {
+              const double cc = (double)cv;
+              const double ed = need_e ? (double)e[p] : 0.0;
+              double o;
+              if (a.measure == kCrossCorr) o = cc;
+              else if (a.measure == kSqrDistance) o = ed - 2.0 * cc + etd;
+              else if (a.measure == kCrossCorrNorm) o = cc * rsqrt(ed * etd);
+              else o = (ed - 2.0 * cc + etd) * rsqrt(ed * etd);
+              outd[p] = o;
+              outf[p] = (float)o;
+            } else {
+              // Exact in int32: each of C, E_S, E_T <= 64 * 64 * 255^2 < 2^28.
+              const int cc = static_cast<int>(cv);
+              const int es = need_e ? static_cast<int>(e[p]) : 0;
+              const int ei = static_cast<int>(etd);
+              const int num =
+                  (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
+              if (a.measure == kCrossCorr || a.measure == kSqrDistance) {
+                outd[p] = (double)num;
+                outf[p] = __int2float_rn(num);
+              } else if ((double)a.tw * a.th * 65025.0 <= 16777216.0) {  // float sums exact
+                outf[p] = __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
+                outd[p] = outf[p];
+              } else {
+                outd[p] = __ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
+                outf[p] = (float)outd[p];
+              }
+            }
           }
-          if (need_e) {
+          const int x0 = a.xs_out + S * m;
+          if (a.nch == 1 && !a.dst_f64 && x0 + S <= a.W) {
+            float* o = reinterpret_cast<float*>(orow) + x0;
+            if (S % 4 == 0) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int rem = a.tw - 16 * c - 4 * j;
-              uint32_t v = __funnelshift_rc(w[j], w[j + 1], sh2);  // sh2 may be 32
-              if (rem <= 0) v = 0;
-              else if (rem < 4) v &= (1u << (8 * rem)) - 1u;
-              acc = __dp4a(v, v, acc);
+              for (int j = 0; j < S / 4; ++j)
+                reinterpret_cast<float4*>(o)[j] = make_float4(
+                    outf[(4 * j) % S], outf[(4 * j + 1) % S], outf[(4 * j + 2) % S],
+                    outf[(4 * j + 3) % S]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < S / 2; ++j)
+                reinterpret_cast<float2*>(o)[j] = make_float2(outf[(2 * j) % S], outf[(2 * j + 1) % S]);
+            }
+          } else {
+#pragma unroll
+            for (int p = 0; p < S; ++p) {
+              const int x = x0 + p;
+              if (x >= a.W) break;
+              const size_t xo = (size_t)x * a.nch + ch;
+              if (a.dst_f64)
+                reinterpret_cast<double*>(orow)[xo] = outd[p];
+              else
+                reinterpret_cast<float*>(orow)[xo] = outf[p];
             }
           }
         }
-        if (need_e) rs = static_cast<ET>(acc);
       }
-      if (need_e) {
-        // Window energy: add this row, drop the row th steps back (the ring
-        // holds R >= th rows; read before write when th == R).
-        ST* slot = rsring + (t & (R - 1)) * kPos + pos;
-        const ST old = t >= a.th ? rsring[((t - a.th) & (R - 1)) * kPos + pos] : ST(0);
-        const ST cur = static_cast<ST>(rs);
-        *slot = cur;
-        ewin += static_cast<ET>(cur) - static_cast<ET>(old);
-        estage[(t & (kNE - 1)) * kPos + pos] = ewin;
-      }
-      tmem_st_wait();
+      // The partial is released only after the block's window energies have
+      // been read: the MMAs then run at most one block ahead of this one and
+      // the builders at most 2 B + kNA steps ahead of it (the energy ring's
+      // depth).
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) {
-        if (need_e) mbar_arrive(&e_full[t & (kNE - 1)]);
-        mbar_arrive(&ready[i]);
-      }
-      if (++i == NS) { i = 0; iph ^= 1; }
-      if (++rr == kRB) { rr = 0; if (++st == kNRaw) { st = 0; rph ^= 1; } }
-    }
-  } else {
-    // ---- Epilogue: running sums over template rows, energies, output ------------
-    // Values used only when a row is written are read from shared memory
-    // (the item, cs.et) at that point, which keeps registers for the R sums.
-    const int ph = (warp - kBuilders) >> 2;  // positions 2m + ph, D columns [ph R, ph R + R)
-    const uint32_t d_col = lane_base + ph * R;
-    AT acc[R];
-#pragma unroll
-    for (int j = 0; j < R; ++j) acc[j] = AT(0);
-    int i = 0;
-    uint32_t iph = 0;
-    for (int s = 0; s < nsteps; ++s) {
-      if (!mbar_wait(&mma_done[i], iph, abort_flag, kSpinLimit)) break;
-      tc_fence_after();
-      // D[n] = column i*N2 + ph*R + n. Chunks are taken from the top so the
-      // shift-add below runs with ascending c (acc[c - 1] <- acc[c] + D[R-1-c]).
-      constexpr int CW = R == 32 ? 32 : 16;  // 16-column loads keep R = 64 in registers
-      AT outv = AT(0);
-#pragma unroll
-      for (int q = R / CW - 1; q >= 0; --q) {
-        uint32_t v[32];
-        if (CW == 32)
-          tmem_ld32(d_col + i * N2 + q * CW, v);
-        else
-          tmem_ld16(d_col + i * N2 + q * CW, v);
-        tmem_ld_wait();
-#pragma unroll
-        for (int j = CW - 1; j >= 0; --j) {
-          const int n = q * CW + j;
-          const int c = R - 1 - n;
-          const AT val = SPLIT ? (AT)__uint_as_float(v[j]) : (AT) static_cast<int>(v[j]);
-          if (c == 0)
-            outv = acc[0] + val;
-          else
-            acc[c - 1] = acc[c] + val;
-        }
-      }
-      acc[R - 1] = AT(0);
-      const int pos = 2 * m + ph;
-      ET e = ET(0);
-      if (need_e) {
-        if (!mbar_wait(&e_full[s & (kNE - 1)], (s / kNE) & 1, abort_flag, kSpinLimit)) break;
-        e = estage[(s & (kNE - 1)) * kPos + pos];
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&ready[i]);  // D stage i free for step s + NS
-      if (++i == NS) { i = 0; iph ^= 1; }
-
-      const int yd = a.y0 + s - R + 1;
-      const int x = a.xs_out + pos;
-      if (s >= R - 1 && yd < a.yend && x < a.W) {
-        const size_t xo = (size_t)x * a.nch + ch;  // element of the score-map row
-        const double etd = cs.et;
-        const ET et = static_cast<ET>(etd);
-        double outd;
-        float outf;
-        if (SPLIT) {
-          const double cc = (double)outv;
-          const double ed = (double)e;
-          if (a.measure == kCrossCorr) outd = cc;
-          else if (a.measure == kSqrDistance) outd = ed - 2.0 * cc + etd;
-          else if (a.measure == kCrossCorrNorm) outd = cc * rsqrt(ed * etd);
-          else outd = (ed - 2.0 * cc + etd) * rsqrt(ed * etd);
-          outf = (float)outd;
-        } else {
-          // Exact in int32: each of C, E_S, E_T <= 64 * 64 * 255^2 < 2^28.
-          const int cc = static_cast<int>(outv);
-          const int es = static_cast<int>(e), ei = static_cast<int>(et);
-          const int num =
-              (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
-          if (a.measure == kCrossCorr || a.measure == kSqrDistance) {
-            outd = (double)num;
-            outf = __int2float_rn(num);
-          } else if ((double)a.tw * a.th * 65025.0 <= 16777216.0) {  // float sums exact
-            outf = __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
-            outd = outf;
-          } else {
-            outd = __ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
-            outf = (float)outd;
-          }
-        }
-        char* o = a.dst + (size_t)yd * a.dst_pitch;
-        if (a.dst_f64)
-          reinterpret_cast<double*>(o)[xo] = outd;
-        else
-          reinterpret_cast<float*>(o)[xo] = outf;
-      }
+      if (lane == 0) mbar_arrive(&buf_free[k & 1]);
+      if (!__all_sync(0xffffffffu, ok)) break;
     }
   }
 
@@ -579,74 +776,43 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   __syncthreads();
   tc_fence_after();
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kNRaw; ++i) mbar_inval(&raw_full[i]);
-    for (int i = 0; i < NS; ++i) {
+    for (int i = 0; i < kNRaw; ++i) {
+      mbar_inval(&raw_full[i]);
+      mbar_inval(&raw_free[i]);
+    }
+    for (int i = 0; i < kNA; ++i) {
       mbar_inval(&ready[i]);
       mbar_inval(&mma_done[i]);
     }
-    for (int i = 0; i < kNE; ++i) mbar_inval(&e_full[i]);
+    for (int i = 0; i < kNE; ++i) {
+      mbar_inval(&e_full[i]);
+      mbar_inval(&e_free[i]);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_inval(&blk_full[i]);
+      mbar_inval(&buf_free[i]);
+    }
     mbar_inval(done_bar);
   }
 }
 
-// Template classes: R in {16, 32, 64} (template rows) x K (template columns
-// + 1, padded to 16 for BF16 / 32 for i8).
+// Template classes: R in {16, 32, 64} (template rows rounded up); the strip
+// width is 128 S positions.
+inline int class_of(int th) { return th <= 16 ? 0 : th <= 32 ? 1 : 2; }
+__host__ __device__ inline int class_r(int cls) { return 16 << cls; }
 template <int ELEM>
-struct Classes {
-  static constexpr int nk = ElemTraits<ELEM>::split ? 5 : 3;
-  static constexpr int kstep = ElemTraits<ELEM>::split ? 16 : 32;
-  static constexpr int kmax = nk * kstep;
-};
-
-template <int ELEM>
-inline int class_of(int tw, int th) {
-  typedef Classes<ELEM> C;
-  const int r = th <= 16 ? 0 : th <= 32 ? 1 : 2;
-  const int k = (tw + 1 + C::kstep - 1) / C::kstep - 1;
-  return r * C::nk + k;
+int strip_width(int cls) {
+  return kM * s_for(class_r(cls));
 }
 
 template <int ELEM>
-__host__ __device__ inline void class_rk(int cls, int* R, int* K) {
-  typedef Classes<ELEM> C;
-  *R = 16 << (cls / C::nk);
-  *K = (cls % C::nk + 1) * C::kstep;
-}
-
-template <int ELEM>
-__device__ __forceinline__ void dispatch(int cls, const ItemArgs& a, unsigned char* smem,
-                                         CtaState& cs) {
-  if constexpr (ElemTraits<ELEM>::split) {
-    switch (cls) {
-      case 0: run_item<ELEM, 16, 16>(a, smem, cs); break;
-      case 1: run_item<ELEM, 16, 32>(a, smem, cs); break;
-      case 2: run_item<ELEM, 16, 48>(a, smem, cs); break;
-      case 3: run_item<ELEM, 16, 64>(a, smem, cs); break;
-      case 4: run_item<ELEM, 16, 80>(a, smem, cs); break;
-      case 5: run_item<ELEM, 32, 16>(a, smem, cs); break;
-      case 6: run_item<ELEM, 32, 32>(a, smem, cs); break;
-      case 7: run_item<ELEM, 32, 48>(a, smem, cs); break;
-      case 8: run_item<ELEM, 32, 64>(a, smem, cs); break;
-      case 9: run_item<ELEM, 32, 80>(a, smem, cs); break;
-      case 10: run_item<ELEM, 64, 16>(a, smem, cs); break;
-      case 11: run_item<ELEM, 64, 32>(a, smem, cs); break;
-      case 12: run_item<ELEM, 64, 48>(a, smem, cs); break;
-      case 13: run_item<ELEM, 64, 64>(a, smem, cs); break;
-      default: run_item<ELEM, 64, 80>(a, smem, cs); break;
-    }
-  } else {
-    switch (cls) {
-      case 0: run_item<ELEM, 16, 32>(a, smem, cs); break;
-      case 1: run_item<ELEM, 16, 64>(a, smem, cs); break;
-      case 2: run_item<ELEM, 16, 96>(a, smem, cs); break;
-      case 3: run_item<ELEM, 32, 32>(a, smem, cs); break;
-      case 4: run_item<ELEM, 32, 64>(a, smem, cs); break;
-      case 5: run_item<ELEM, 32, 96>(a, smem, cs); break;
-      case 6: run_item<ELEM, 64, 32>(a, smem, cs); break;
-      case 7: run_item<ELEM, 64, 64>(a, smem, cs); break;
-      default: run_item<ELEM, 64, 96>(a, smem, cs); break;
-    }
-  }
+__device__ __forceinline__ void dispatch(const ItemArgs& a, unsigned char* smem, CtaState& cs) {
+  if (a.R == 16)
+    run_item<ELEM, 8>(a, smem, cs);
+  else if (a.R == 32)
+    run_item<ELEM, 4>(a, smem, cs);
+  else
+    run_item<ELEM, 2>(a, smem, cs);
 }
 
 // Batch tables (device memory).
@@ -656,7 +822,7 @@ struct BatchImage {
 struct BatchTemplate {
   const char* ptr;
   size_t pitch;
-  int tw, th, cls;
+  int tw, th, cls;  // cls: template rows class (R = 16 << cls)
 };
 struct BatchDest {
   char* ptr;
@@ -676,7 +842,7 @@ struct TensorLaunch {
   int* err;
   // mode 0
   ItemArgs base;       // fields common to every item
-  int cls, BH;
+  int BH;
   // mode 1
   const CUtensorMap* maps;  // one per image (64-byte aligned)
   const BatchImage* imgs;
@@ -705,18 +871,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   // The item's arguments live in shared memory: read where they are used,
   // they take no registers from the roles' accumulators.
   __shared__ ItemArgs item;
-  __shared__ int item_cls;
   if (P.mode == 0) {
     if (threadIdx.x == 0) {
       item = P.base;
       item.tmap = &P.map;
       item.ch = blockIdx.z;
-      item.xs_out = blockIdx.x * kPos;
+      item.xs_out = blockIdx.x * kM * s_for(item.R);
       item.y0 = blockIdx.y * P.BH;
       item.yend = min(item.H, item.y0 + P.BH);
     }
     __syncthreads();
-    dispatch<ELEM>(P.cls, item, smem, cs);
+    dispatch<ELEM>(item, smem, cs);
   } else {
     for (;;) {
       if (threadIdx.x == 0) {
@@ -732,11 +897,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.H = im.H;
           item.tw = tp.tw;
           item.th = tp.th;
+          item.R = class_r(tp.cls);
           item.ax = tp.tw / 2;
           item.ay = tp.th / 2;
           item.nch = im.nch;
           item.ch = bi.ch;
-          item.xs_out = bi.strip * kPos;
+          item.xs_out = bi.strip * kM * s_for(item.R);
           item.y0 = bi.y0;
           item.yend = bi.yend;
           item.nbox = P.nbox;
@@ -746,13 +912,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.dst_pitch = ds.pitch;
           item.dst_f64 = ds.f64;
           item.measure = P.measure;
-          item_cls = tp.cls;
         }
       }
       __syncthreads();
       const int it = cs.next;
       if (it >= P.nitems) break;
-      dispatch<ELEM>(item_cls, item, smem, cs);
+      dispatch<ELEM>(item, smem, cs);
       __syncthreads();  // every thread has read the item before it is replaced
     }
   }
@@ -818,18 +983,39 @@ int band_height(int H, int R, long long columns, int sm_count) {
   return best_bh;
 }
 
+// Lead of the staged row (elements before the first window pixel, so that
+// the TMA copy starts on a 16-byte group).
 template <int ELEM>
-int nbox_for(int K) {
+int lead_for(int ax) {
+  const int inner = ElemTraits<ELEM>::inner;
+  return (inner - ax % inner) % inner;
+}
+
+template <int ELEM>
+Geo geo_for(int cls, int tw, int ax) {
+  return make_geo(ElemTraits<ELEM>::split, class_r(cls), tw, lead_for<ELEM>(ax));
+}
+
+// 16-byte groups a staged row needs for a template of this class and width.
+template <int ELEM>
+int nbox_for(int cls, int tw, int ax) {
   typedef ElemTraits<ELEM> TR;
-  // Lane m reads pixels lead + 2m .. lead + 2m + K (one more for odd leads).
-  return (kPos + K + 2 * TR::inner + 1) / TR::inner;
+  const Geo g = geo_for<ELEM>(cls, tw, ax);
+  return (staged_elems(g, TR::split) + TR::inner - 1) / TR::inner;
+}
+
+template <int ELEM>
+int smem_for(int cls, int tw, int ax, int nbox) {
+  return std::max(make_layout(ElemTraits<ELEM>::split, geo_for<ELEM>(cls, tw, ax), nbox).total,
+                  kMinSmem);
 }
 
 // Rank-4 view of source planes: 16-byte groups (dim 0), groups along the row
-// (dim 1), rows (dim 2), channels (dim 3). A staged row of 256 + K pixels is
-// one box of nbox groups, under the 256-element box limit. The last group of
-// a row may reach into the row pitch, which is zero (image creation
-// zero-fills device buffers; the channel split writes zeros there).
+// (dim 1), rows (dim 2), channels (dim 3). A staged row (the strip plus the
+// template width, nbox groups) is box_split(nbox) boxes of box_part(nbox)
+// groups and one row. The last group of a row may reach into the row pitch,
+// which is zero (image creation zero-fills device buffers; the channel split
+// writes zeros there).
 template <int ELEM>
 cudaError_t encode_planes(CUtensorMap* map, const void* planes, int W, int H, int nch,
                           size_t plane_pitch, size_t plane_bytes, int nbox) {
@@ -842,7 +1028,7 @@ cudaError_t encode_planes(CUtensorMap* map, const void* planes, int W, int H, in
   const cuuint64_t gdim[4] = {(cuuint64_t)TR::inner, (cuuint64_t)((W + TR::inner - 1) / TR::inner),
                               (cuuint64_t)H, (cuuint64_t)nch};
   const cuuint64_t gstride[3] = {16, (cuuint64_t)plane_pitch, (cuuint64_t)plane_bytes};
-  const cuuint32_t box[4] = {(cuuint32_t)TR::inner, (cuuint32_t)nbox, (cuuint32_t)kRB, 1};
+  const cuuint32_t box[4] = {(cuuint32_t)TR::inner, (cuuint32_t)box_part(nbox), 1, 1};
   const cuuint32_t estride[4] = {1, 1, 1, 1};
   CUresult r = enc(map, dt, 4, const_cast<void*>(planes), gdim, gstride, box, estride,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -875,32 +1061,27 @@ size_t plane_set_bytes(const DevImage& s) {
 }
 
 template <int ELEM>
-int smem_for_class(int cls, int nbox) {
-  int R, K;
-  class_rk<ELEM>(cls, &R, &K);
-  return std::max(make_layout(ElemTraits<ELEM>::split, R, K, nbox).total, kMinSmem);
-}
-
-template <int ELEM>
 cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevImage& tmpl,
                        const DevImage& dst, int ax, int ay) {
-  const int cls = class_of<ELEM>(tmpl.width, tmpl.height);
-  int R, K;
-  class_rk<ELEM>(cls, &R, &K);
+  const int cls = class_of(tmpl.height);
+  const int R = class_r(cls);
   TensorLaunch P;
   std::memset(&P, 0, sizeof(P));
   P.mode = 0;
   P.measure = m;
-  P.nbox = nbox_for<ELEM>(K);
+  P.nbox = nbox_for<ELEM>(cls, tmpl.width, ax);
   P.err = reinterpret_cast<int*>(ctx.scratch(Context::kTensorAux, 256));
-  P.cls = cls;
-  const int nstrips = (src.width + kPos - 1) / kPos;
-  P.BH = band_height(src.height, R, (long long)nstrips * src.nch, ctx.sm_count);
+  const int sw = strip_width<ELEM>(cls);
+  const int nstrips = (src.width + sw - 1) / sw;
+  P.BH = ctx.band_rows > 0
+             ? std::min(ctx.band_rows, src.height)
+             : band_height(src.height, R, (long long)nstrips * src.nch, ctx.sm_count);
   ItemArgs& a = P.base;
   a.W = src.width;
   a.H = src.height;
   a.tw = tmpl.width;
   a.th = tmpl.height;
+  a.R = R;
   a.ax = ax;
   a.ay = ay;
   a.nch = src.nch;
@@ -911,6 +1092,9 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
   a.dst_pitch = dst.pitch;
   a.dst_f64 = dst.type == F64;
   a.measure = m;
+
+  const int smem_bytes = smem_for<ELEM>(cls, tmpl.width, ax, P.nbox);
+  if (smem_bytes > kMaxDynSmem) return cudaErrorInvalidValue;
 
   // Source planes: the image itself for one channel, else a split copy.
   const void* planes = src.ptr;
@@ -924,7 +1108,6 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
                                       plane_pitch, plane_pitch * src.height, P.nbox);
   if (e != cudaSuccess) return e;
 
-  const int smem_bytes = smem_for_class<ELEM>(cls, P.nbox);
   auto kern = prox_tensor_kernel<ELEM>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            kMaxDynSmem);
@@ -991,11 +1174,12 @@ std::vector<BatchItem> make_items(const std::vector<DevImage>& imgs,
   for (size_t p = 0; p < pair_img.size(); ++p) {
     const DevImage& s = imgs[pair_img[p]];
     const DevImage& t = tpls[pair_tpl[p]];
-    const int cls = class_of<ELEM>(t.width, t.height);
-    int R, K;
-    class_rk<ELEM>(cls, &R, &K);
+    const int cls = class_of(t.height);
+    const int R = class_r(cls);
+    const Geo g = geo_for<ELEM>(cls, t.width, t.width / 2);
     const int BH = bh.at(cls);
-    const int nstrips = (s.width + kPos - 1) / kPos;
+    const int sw = strip_width<ELEM>(cls);
+    const int nstrips = (s.width + sw - 1) / sw;
     for (int c = 0; c < s.nch; ++c)
       for (int st = 0; st < nstrips; ++st)
         for (int y0 = 0; y0 < s.height; y0 += BH) {
@@ -1007,8 +1191,8 @@ std::vector<BatchItem> make_items(const std::vector<DevImage>& imgs,
           it.strip = st;
           it.y0 = y0;
           it.yend = std::min(s.height, y0 + BH);
-          // steps x MMA work per step (K columns, plus a fixed part)
-          const long long cost = (long long)(it.yend - y0 + R - 1) * (K + 64);
+          // steps x MMA work per step (MMAs of Np columns, plus a fixed part)
+          const long long cost = (long long)(it.yend - y0 + R - 1) * (g.nmma * kNp + 512);
           v.push_back({cost, it});
         }
   }
@@ -1071,14 +1255,15 @@ cudaError_t upload_tables(TensorBatch& b, const std::vector<CUtensorMap>& maps,
 // bands) and load balance (favouring short ones).
 template <int ELEM>
 int autotune_bh(Context& ctx, int measure, const DevImage& img, const CUtensorMap& map,
-                const DevImage& tpl, int cls, int nbox, char* probe_dst, size_t probe_pitch) {
-  int R, K;
-  class_rk<ELEM>(cls, &R, &K);
+                const DevImage& tpl, int cls, int nbox, int smem, char* probe_dst,
+                size_t probe_pitch) {
+  const int R = class_r(cls);
   std::vector<int> cand;
   for (int bh : {64, 128, 192, 256, 384, 512, 768, 1024})
     if (bh >= R && bh < img.height) cand.push_back(bh);
   cand.push_back(img.height);
-  const int nstrips = (img.width + kPos - 1) / kPos;
+  const int sw = strip_width<ELEM>(cls);
+  const int nstrips = (img.width + sw - 1) / sw;
   const long long units = (long long)nstrips * img.nch;
   // Replicas so that the shortest candidate has at least 4 items per SM.
   const int min_bh = cand.front();
@@ -1106,7 +1291,7 @@ int autotune_bh(Context& ctx, int measure, const DevImage& img, const CUtensorMa
     tb.launch.measure = measure;
     tb.launch.nbox = nbox;
     tb.launch.err = reinterpret_cast<int*>(ctx.scratch(Context::kTensorAux, 256));
-    tb.smem = smem_for_class<ELEM>(cls, nbox);
+    tb.smem = smem;
     void* mem = nullptr;
     if (upload_tables<ELEM>(tb, maps, bimgs, btpls, bdsts, items, &mem) != cudaSuccess) break;
     float ms = 1e30f;
@@ -1134,12 +1319,14 @@ template <int ELEM>
 TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& imgs,
                           const std::vector<DevImage>& tpls, const std::vector<DevImage>& dsts,
                           cudaError_t* err) {
-  typedef Classes<ELEM> C;
   TensorBatch* b = new TensorBatch();
   b->ctx = &ctx;
   b->elem = ELEM;
   b->measure = m;
-  b->nbox = nbox_for<ELEM>(C::kmax);
+  // One staged-row width for every tensor map of the batch: the widest need.
+  b->nbox = 1;
+  for (const DevImage& t : tpls)
+    b->nbox = std::max(b->nbox, nbox_for<ELEM>(class_of(t.height), t.width, t.width / 2));
   b->images = imgs;
   std::memset(&b->launch, 0, sizeof(b->launch));
   cudaError_t e = cudaSuccess;
@@ -1177,13 +1364,21 @@ TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& 
   std::vector<BatchTemplate> btpls;
   for (const DevImage& t : tpls)
     btpls.push_back(BatchTemplate{(const char*)t.ptr, t.pitch, t.width, t.height,
-                                  class_of<ELEM>(t.width, t.height)});
+                                  class_of(t.height)});
   std::vector<BatchDest> bdsts;
   for (const DevImage& d : dsts) bdsts.push_back(BatchDest{(char*)d.ptr, d.pitch, d.type == F64});
 
   auto kern = prox_tensor_kernel<ELEM>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (e != cudaSuccess) return fail(e);
+  // Shared memory: the largest need of any template (per class, the widest).
+  std::map<int, int> cls_smem;
+  for (const DevImage& t : tpls) {
+    const int c = class_of(t.height);
+    const int sm = smem_for<ELEM>(c, t.width, t.width / 2, b->nbox);
+    if (sm > kMaxDynSmem) return fail(cudaErrorInvalidValue);
+    cls_smem[c] = std::max(cls_smem[c], sm);
+  }
 
   // Multi-channel probes read the planes: split them once before tuning.
   for (size_t i = 0; i < imgs.size(); ++i)
@@ -1210,7 +1405,8 @@ TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& 
     const size_t pp = ((size_t)probe.width * probe.nch * 4 + 127) / 128 * 128;
     e = cudaMalloc(&pd, pp * probe.height);
     if (e != cudaSuccess) return fail(e);
-    const int v = autotune_bh<ELEM>(ctx, m, probe, maps[0], tpls[j], cls, b->nbox, pd, pp);
+    const int v = autotune_bh<ELEM>(ctx, m, probe, maps[0], tpls[j], cls, b->nbox,
+                                    cls_smem[cls], pd, pp);
     cudaStreamSynchronize(ctx.stream);
     cudaFree(pd);
     e = cudaGetLastError();
@@ -1237,7 +1433,7 @@ TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& 
   if (e != cudaSuccess) return fail(e);
   b->nitems = b->launch.nitems;
   b->smem = 0;
-  for (const auto& kv : bh) b->smem = std::max(b->smem, smem_for_class<ELEM>(kv.first, b->nbox));
+  for (const auto& kv : cls_smem) b->smem = std::max(b->smem, kv.second);
 
   // Capture the batch (splits, queue reset, persistent launch) as a graph.
   e = cudaStreamSynchronize(ctx.stream);
@@ -1328,10 +1524,8 @@ cudaError_t tensor_batch_run(TensorBatch* b) {
 int tensor_batch_items(const TensorBatch* b) { return b->nitems; }
 
 int tensor_batch_band_height(const TensorBatch* b, int tw, int th) {
-  int cls = 0;
-  if (b->elem == kU8) cls = class_of<kU8>(tw, th);
-  else cls = class_of<kF32>(tw, th);
-  auto it = b->bh.find(cls);
+  (void)tw;
+  auto it = b->bh.find(class_of(th));
   return it == b->bh.end() ? 0 : it->second;
 }
 

@@ -90,6 +90,7 @@ def _load():
         "ocipSetProximityPath": (i32, [ctypes.c_int]),
         "ocipGetProximityPath": (i32, [ctypes.POINTER(ctypes.c_int)]),
         "ocipGetLastProximityPath": (i32, [ctypes.POINTER(ctypes.c_int)]),
+        "ocipSetProximityBandHeight": (i32, [ctypes.c_int]),
         "ocipGetLastErrorMessage": (ctypes.c_char_p, []),
         "ocipGetStream": (i32, [ctypes.POINTER(vp)]),
         "ocipGetImageDevicePtr": (i32, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t)]),
@@ -164,6 +165,9 @@ class Context:
 
     def set_path(self, path):
         check(lib.ocipSetProximityPath(path), "ocipSetProximityPath")
+
+    def set_band_height(self, rows):
+        check(lib.ocipSetProximityBandHeight(rows), "ocipSetProximityBandHeight")
 
     def last_path(self):
         v = ctypes.c_int()

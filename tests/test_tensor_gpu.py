@@ -276,6 +276,42 @@ def test_cfg5_u16_full_size_accuracy_on_crops(ocip, ctx):
     ctx.set_path(ocip.PATH_PLAIN)
 
 
+@pytest.mark.parametrize("dtype,th,tw,nch", [(np.float32, 16, 16, 1), (np.float32, 31, 31, 1),
+                                             (np.float32, 64, 64, 1), (np.float32, 48, 33, 1),
+                                             (np.uint16, 40, 48, 2), (np.uint8, 24, 24, 1),
+                                             (np.uint8, 64, 64, 3)])
+def test_tall_bands_slide_through_epochs(ocip, ctx, dtype, th, tw, nch):
+    """One work item per strip covering all 420 rows: the accumulator window
+    slides to the end of its TMEM region several times (open rows copied
+    down, the columns after them cleared). U8 stays bit-identical to the
+    plain path; F32 and U16 stay within the 1e-5 bar."""
+    ctx.make_current()
+    rng = np.random.default_rng(th * 31 + tw + nch)
+    H, W = 420, 200 if th > 32 else 300
+    shape = (H, W, nch) if nch > 1 else (H, W)
+    tshape = (th, tw, nch) if nch > 1 else (th, tw)
+    if dtype == np.float32:
+        S = rng.random(shape).astype(np.float32)
+        T = rng.random(tshape).astype(np.float32)
+    else:
+        hi = 256 if dtype == np.uint8 else 65536
+        S = rng.integers(0, hi, shape, dtype=dtype)
+        T = rng.integers(0, hi, tshape, dtype=dtype)
+    ctx.set_band_height(H)
+    try:
+        for m in (0, 1, 3, 4):
+            got, path = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
+            assert path == ocip.PATH_TENSOR
+            if dtype == np.uint8:
+                plain, _ = run(ocip, ctx, m, S, T, ocip.PATH_PLAIN)
+                assert np.array_equal(plain, got, equal_nan=True), MEAS[m]
+            else:
+                f32_check(got, S, T, m)
+    finally:
+        ctx.set_band_height(0)
+        ctx.set_path(ocip.PATH_PLAIN)
+
+
 def test_bounded_wait_expires_and_context_stays_usable(ocip, ctx):
     """A kernel waits on a barrier nothing arrives on: the bounded wait
     expires (about 1 ms here), the kernel returns, the error surfaces as
