@@ -50,20 +50,20 @@
 //
 // Window energy sum S^2 of each position: per source row the energy warps sum
 // tw squares per position (FP32 FMA for F32, exact integers for U8 and U16;
-// the S positions of a thread are independent chains), keep the row sums in a
+// the positions of a thread are independent chains), keep the row sums in a
 // ring of R rows and a running sum over the last th rows (FP64 or exact
 // integers) and hand the window sums to the epilogue through a ring in shared
 // memory whose entries the epilogue releases. SqrDistance = E_S - 2C + E_T and the _Norm scale are
 // done in FP64 (F32, U16) or as the plain path does them (U8: the results are
 // bit-identical to it).
 //
-// Roles (14 warps; one CTA per SM, which holds all 512 TMEM columns):
+// Roles (18 warps; one CTA per SM, which holds all 512 TMEM columns):
 //   warps 0-3  builders: the A operand of each row (split into hi/lo);
 //   warps 4-7  epilogue (warp 4 + k reads TMEM lanes 32k .. 32k + 31): running
 //              sums in the TMEM ring, score map;
 //   warp 8     TMA loads of source rows (zero fill outside the image);
 //   warp 9     MMA issue (one commit per source row, one per block);
-//   warps 10-13 window energies (measures other than CrossCorr).
+//   warps 10-17 window energies (measures other than CrossCorr).
 // Every wait is bounded: a wait that gives up sets the CTA's abort flag, the
 // roles leave their loops, the MMA and TMA threads drain what they issued,
 // and the kernel raises the context's error flag.
@@ -94,7 +94,7 @@ constexpr int kEpilogue = 4;
 constexpr int kTmaWarp = kBuilders + kEpilogue;
 constexpr int kMmaWarp = kTmaWarp + 1;
 constexpr int kEnergyWarp = kMmaWarp + 1;  // first of the window-energy warps
-constexpr int kEnergy = 4;
+constexpr int kEnergy = 8;
 constexpr int kThreads = (kEnergyWarp + kEnergy) * 32;
 constexpr int kBuildThreads = kBuilders * 32;
 constexpr int kNRaw = 6;                // staged source rows (TMA stages of one row)
@@ -110,6 +110,7 @@ constexpr int kMinSmem = 120 * 1024;    // keeps one CTA per SM (it takes all of
 constexpr int kMaxDynSmem = 226 * 1024; // opt-in dynamic shared memory limit of the kernel
 constexpr long long kSpinLimit = 4000000000LL;  // about 2 s of SM clock
 constexpr int kBarBuild = 1;            // named barrier of the builder warps
+constexpr int kEnergyThreads = kEnergy * 32;
 
 enum Elem { kF32 = 0, kU8 = 1, kU16 = 2 };
 
@@ -327,7 +328,7 @@ __device__ __forceinline__ bool builders_all(bool p) {
   return r != 0;
 }
 
-// Runs one work item with all 14 warps of the CTA. The caller has
+// Runs one work item with all 18 warps of the CTA. The caller has
 // synchronised the CTA; TMEM (512 columns) is allocated. Barriers are
 // initialised here and invalidated at the end, so consecutive items may use
 // different layouts.
@@ -569,17 +570,20 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     }
   } else if (warp >= kEnergyWarp) {
     // ---- Window energies ----------------------------------------------------------
-    // Positions x = b + 128 p: row sum of tw squares from staged element
-    // lead + x (the S positions of a thread are independent chains); the window
-    // sum adds this row and drops the row th steps back (the ring holds
-    // R >= th rows; read before write when th == R).
+    // Thread b handles positions x = b + 256 p (p < S / 2): row sum of tw
+    // squares from staged element lead + x (its positions are independent
+    // chains; a warp reads consecutive elements); the window sum adds this
+    // row and drops the row th steps back (the ring holds R >= th rows; read
+    // before write when th == R).
     if (need_e) {
-      const int b = threadIdx.x - kEnergyWarp * 32;  // 0 .. 127
+      constexpr int SE = S / 2;  // positions per energy thread
+      const int b = threadIdx.x - kEnergyWarp * 32;  // 0 .. 255
+      const int tw = a.tw, th = a.th;  // registers: the item lives in shared memory
       ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
       ST* estage = reinterpret_cast<ST*>(smem + L.es);
-      WT ewin[S];
+      WT ewin[SE];
 #pragma unroll
-      for (int p = 0; p < S; ++p) ewin[p] = WT(0);
+      for (int p = 0; p < SE; ++p) ewin[p] = WT(0);
       int st = 0;
       uint32_t rph = 0;
       for (int t = 0; t < nsteps; ++t) {
@@ -590,26 +594,26 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         if (!__all_sync(0xffffffffu, ok)) break;
         const unsigned char* row = smem + L.raw + st * L.raw_stage;
         ST* es = estage + ei * P;
-        RT rs[S];
+        RT rs[SE];
 #pragma unroll
-        for (int p = 0; p < S; ++p) rs[p] = RT(0);
+        for (int p = 0; p < SE; ++p) rs[p] = RT(0);
         const int e0 = lead + b;
         int w = 0;
-        for (; w + 4 <= a.tw; w += 4) {
+        for (; w + 8 <= tw; w += 8) {
 #pragma unroll
-          for (int d = 0; d < 4; ++d)
+          for (int d = 0; d < 8; ++d)
 #pragma unroll
-            for (int p = 0; p < S; ++p) rs[p] += sq_at<ELEM>(row, e0 + kBuildThreads * p + w + d);
+            for (int p = 0; p < SE; ++p) rs[p] += sq_at<ELEM>(row, e0 + kEnergyThreads * p + w + d);
         }
-        for (; w < a.tw; ++w) {
+        for (; w < tw; ++w) {
 #pragma unroll
-          for (int p = 0; p < S; ++p) rs[p] += sq_at<ELEM>(row, e0 + kBuildThreads * p + w);
+          for (int p = 0; p < SE; ++p) rs[p] += sq_at<ELEM>(row, e0 + kEnergyThreads * p + w);
         }
 #pragma unroll
-        for (int p = 0; p < S; ++p) {
-          const int x = b + kBuildThreads * p;
+        for (int p = 0; p < SE; ++p) {
+          const int x = b + kEnergyThreads * p;
           ST* slot = rsring + (t & (R - 1)) * P + x;
-          const ST old = t >= a.th ? rsring[((t - a.th) & (R - 1)) * P + x] : ST(0);
+          const ST old = t >= th ? rsring[((t - th) & (R - 1)) * P + x] : ST(0);
           const ST cur = static_cast<ST>(rs[p]);
           *slot = cur;
           ewin[p] += static_cast<WT>(cur) - static_cast<WT>(old);
@@ -632,6 +636,52 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     const uint32_t ring = lane_base + kRingCol;
     const ST* estage = reinterpret_cast<const ST*>(smem + L.es);
     const double etd = cs.et;
+    const float ret = (float)(1.0 / sqrt(etd));  // 1 / sqrt(E_T)
+    // Score of one position from its product sum cv and window energy ev.
+    // Split sources: SqrDistance's terms cancel near a match, so its
+    // numerator is formed in FP64; the _Norm scale of an F32 map is taken in
+    // FP32 (relative error a few 1e-7), of an F64 map in FP64. U8: exact
+    // integers and the plain path's float or double formulas (bit-identical).
+    auto num_of = [&](AT cv, ST ev) -> double {
+      const double cc = (double)cv;
+      if (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) return cc;
+      return (double)ev - 2.0 * cc + etd;
+    };
+    auto score_f = [&](AT cv, ST ev) -> float {
+      if (SPLIT) {
+        const double num = num_of(cv, ev);
+        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return (float)num;
+        return (float)num * (rsqrtf((float)ev) * ret);
+      } else {
+        // Exact in int32: each of C, E_S, E_T <= 64 * 64 * 255^2 < 2^28.
+        const int cc = static_cast<int>(cv);
+        const int es = static_cast<int>(ev);
+        const int ei = static_cast<int>(etd);
+        const int num =
+            (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
+        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return __int2float_rn(num);
+        if ((double)a.tw * a.th * 65025.0 <= 16777216.0)  // float sums exact
+          return __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
+        return (float)__ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
+      }
+    };
+    auto score_d = [&](AT cv, ST ev) -> double {
+      if (SPLIT) {
+        const double num = num_of(cv, ev);
+        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return num;
+        return num * rsqrt((double)ev * etd);
+      } else {
+        const int cc = static_cast<int>(cv);
+        const int es = static_cast<int>(ev);
+        const int ei = static_cast<int>(etd);
+        const int num =
+            (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
+        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return (double)num;
+        if ((double)a.tw * a.th * 65025.0 <= 16777216.0)
+          return (double)__fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
+        return __ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
+      }
+    };
     uint32_t zero[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) zero[j] = 0u;
@@ -680,6 +730,10 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         tmem_st16(rc, zero);
       }
       tmem_st_wait();
+      // The partial has been read: the MMAs may refill it (block k + 2).
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&buf_free[k & 1]);
 #pragma unroll
       for (int g = 0; g < BS; ++g) {
         const int u = t0 + g;
@@ -688,6 +742,8 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         // Every step's energy entry is waited for and released in order, so
         // the ring's barriers never run two phases apart.
         ST e[S];
+#pragma unroll
+        for (int p = 0; p < S; ++p) e[p] = ST(0);
         if (need_e) {
           ok = mbar_wait(&e_full[u % kNE], (u / kNE) & 1, abort_flag, kSpinLimit);
           if (!__all_sync(0xffffffffu, ok)) break;
@@ -699,42 +755,11 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         }
         if (u >= R - 1 && yd < a.yend) {
           char* orow = a.dst + (size_t)yd * a.dst_pitch;
-          float outf[S];
-          double outd[S];
-#pragma unroll
-          for (int p = 0; p < S; ++p) {
-            const AT cv = val[g * S + p];
-            if (SPLIT) {
-              const double cc = (double)cv;
-              const double ed = need_e ? (double)e[p] : 0.0;
-              double o;
-              if (a.measure == kCrossCorr) o = cc;
-              else if (a.measure == kSqrDistance) o = ed - 2.0 * cc + etd;
-              else if (a.measure == kCrossCorrNorm) o = cc * rsqrt(ed * etd);
-              else o = (ed - 2.0 * cc + etd) * rsqrt(ed * etd);
-              outd[p] = o;
-              outf[p] = (float)o;
-            } else {
-              // Exact in int32: each of C, E_S, E_T <= 64 * 64 * 255^2 < 2^28.
-              const int cc = static_cast<int>(cv);
-              const int es = need_e ? static_cast<int>(e[p]) : 0;
-              const int ei = static_cast<int>(etd);
-              const int num =
-                  (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
-              if (a.measure == kCrossCorr || a.measure == kSqrDistance) {
-                outd[p] = (double)num;
-                outf[p] = __int2float_rn(num);
-              } else if ((double)a.tw * a.th * 65025.0 <= 16777216.0) {  // float sums exact
-                outf[p] = __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
-                outd[p] = outf[p];
-              } else {
-                outd[p] = __ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
-                outf[p] = (float)outd[p];
-              }
-            }
-          }
           const int x0 = a.xs_out + S * m;
           if (a.nch == 1 && !a.dst_f64 && x0 + S <= a.W) {
+            float outf[S];
+#pragma unroll
+            for (int p = 0; p < S; ++p) outf[p] = score_f(val[g * S + p], e[p]);
             float* o = reinterpret_cast<float*>(orow) + x0;
             if (S % 4 == 0) {
 #pragma unroll
@@ -754,20 +779,13 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
               if (x >= a.W) break;
               const size_t xo = (size_t)x * a.nch + ch;
               if (a.dst_f64)
-                reinterpret_cast<double*>(orow)[xo] = outd[p];
+                reinterpret_cast<double*>(orow)[xo] = score_d(val[g * S + p], e[p]);
               else
-                reinterpret_cast<float*>(orow)[xo] = outf[p];
+                reinterpret_cast<float*>(orow)[xo] = score_f(val[g * S + p], e[p]);
             }
           }
         }
       }
-      // The partial is released only after the block's window energies have
-      // been read: the MMAs then run at most one block ahead of this one and
-      // the builders at most 2 B + kNA steps ahead of it (the energy ring's
-      // depth).
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&buf_free[k & 1]);
       if (!__all_sync(0xffffffffu, ok)) break;
     }
   }

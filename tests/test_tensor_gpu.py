@@ -280,11 +280,11 @@ def test_cfg5_u16_full_size_accuracy_on_crops(ocip, ctx):
                                              (np.float32, 64, 64, 1), (np.float32, 48, 33, 1),
                                              (np.uint16, 40, 48, 2), (np.uint8, 24, 24, 1),
                                              (np.uint8, 64, 64, 3)])
-def test_tall_bands_slide_through_epochs(ocip, ctx, dtype, th, tw, nch):
-    """One work item per strip covering all 420 rows: the accumulator window
-    slides to the end of its TMEM region several times (open rows copied
-    down, the columns after them cleared). U8 stays bit-identical to the
-    plain path; F32 and U16 stay within the 1e-5 bar."""
+def test_tall_bands_many_blocks(ocip, ctx, dtype, th, tw, nch):
+    """One work item per strip covering all 420 rows: the running sums go
+    round their TMEM ring many times and the energy ring is reused many times.
+    U8 stays bit-identical to the plain path; F32 and U16 stay within the
+    1e-5 bar."""
     ctx.make_current()
     rng = np.random.default_rng(th * 31 + tw + nch)
     H, W = 420, 200 if th > 32 else 300
