@@ -48,12 +48,13 @@
 // number of additions, so the chains of a whole window (th rows x K chunks)
 // would cost accuracy.
 //
-// Window energy sum S^2 of each position: per source row the energy warps sum
-// tw squares per position (FP32 FMA for F32, exact integers for U8 and U16;
-// the positions of a thread are independent chains), keep the row sums in a
-// ring of R rows and a running sum over the last th rows (FP64 or exact
-// integers) and hand the window sums to the epilogue through a ring in shared
-// memory whose entries the epilogue releases. SqrDistance = E_S - 2C + E_T and the _Norm scale are
+// Window energy sum S^2 of each position: per source row the energy warps
+// square every staged pixel once (FP32 for F32, exact integers for U8 and
+// U16), take each position's row sum of tw squares as the difference of a
+// short running prefix over the thread's S/2 consecutive positions, keep the
+// row sums in a ring of R rows and a running sum over the last th rows (FP64
+// or exact integers) and hand the window sums to the epilogue through a ring
+// in shared memory whose entries the epilogue releases. SqrDistance = E_S - 2C + E_T and the _Norm scale are
 // done in FP64 (F32, U16) or as the plain path does them (U8: the results are
 // bit-identical to it).
 //
@@ -111,6 +112,7 @@ constexpr int kMaxDynSmem = 226 * 1024; // opt-in dynamic shared memory limit of
 constexpr long long kSpinLimit = 4000000000LL;  // about 2 s of SM clock
 constexpr int kBarBuild = 1;            // named barrier of the builder warps
 constexpr int kEnergyThreads = kEnergy * 32;
+constexpr int kBarEnergy = 2;           // named barrier of the energy warps
 
 enum Elem { kF32 = 0, kU8 = 1, kU16 = 2 };
 
@@ -204,7 +206,7 @@ struct ItemArgs {
 
 // Shared-memory layout, identical on host and device.
 struct Layout {
-  int row_bytes, raw_stage, raw, b, a_stage, a, rs, es, bars, total;
+  int row_bytes, raw_stage, raw, b, a_stage, a, rs, es, sq, bars, total;
 };
 
 __host__ __device__ inline int align128(int x) { return (x + 127) & ~127; }
@@ -228,7 +230,10 @@ __host__ __device__ inline Layout make_layout(bool split, const Geo& g, int nbox
   L.a_stage = align128(g.QR * 16 * (split ? 2 : 1));
   L.rs = L.a + kNA * L.a_stage;
   L.es = L.rs + g.R * g.P * 4;
-  L.bars = L.es + g.kNE * g.P * 4;
+  L.sq = L.es + g.kNE * g.P * 4;
+  // Squares of one staged row (8-byte entries at most), padded for the
+  // energy threads' last vector loads.
+  L.bars = L.sq + align128((g.P + 64 + 32) * 8);
   // raw full, raw free; ready, MMA done; energy full, energy free (16 each
   // at most); block full, buffer free; done.
   L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNA + 32 + 4 + 1));
@@ -315,6 +320,36 @@ __device__ __forceinline__ void load8(const unsigned char* row, int e0, float (&
 }
 
 // AND of `p` over the builder warps (a named barrier every builder reaches).
+__device__ __forceinline__ void energy_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(kBarEnergy), "n"(kEnergyThreads) : "memory");
+}
+
+// N consecutive elements of T from an address aligned to N * sizeof(T).
+template <typename T, int N>
+struct Vec {
+  T v[N];
+};
+template <typename T, int N>
+__device__ __forceinline__ Vec<T, N> load_vec(const T* p) {
+  static_assert(N * sizeof(T) <= 32, "vector too wide");
+  Vec<T, N> r;
+  if (N * sizeof(T) == 32) {
+    const uint4 a = reinterpret_cast<const uint4*>(p)[0];
+    const uint4 b = reinterpret_cast<const uint4*>(p)[1];
+    uint4* o = reinterpret_cast<uint4*>(&r);
+    o[0] = a;
+    o[1] = b;
+  } else if (N * sizeof(T) == 16) {
+    *reinterpret_cast<uint4*>(&r) = *reinterpret_cast<const uint4*>(p);
+  } else if (N * sizeof(T) == 8) {
+    *reinterpret_cast<uint2*>(&r) = *reinterpret_cast<const uint2*>(p);
+  } else {
+#pragma unroll
+    for (int j = 0; j < N; ++j) r.v[j] = p[j];
+  }
+  return r;
+}
+
 __device__ __forceinline__ bool builders_all(bool p) {
   uint32_t r;
   asm volatile(
@@ -570,20 +605,28 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     }
   } else if (warp >= kEnergyWarp) {
     // ---- Window energies ----------------------------------------------------------
-    // Thread b handles positions x = b + 256 p (p < S / 2): row sum of tw
-    // squares from staged element lead + x (its positions are independent
-    // chains; a warp reads consecutive elements); the window sum adds this
-    // row and drops the row th steps back (the ring holds R >= th rows; read
-    // before write when th == R).
+    // Per staged row the squares V_k = S^2(lead + k) are written once to a
+    // buffer; thread b then takes the SE = S / 2 consecutive positions
+    // x = SE b + i and streams V_{SE b} .. with aligned vector loads, keeping a
+    // running prefix: the row sum of position x is prefix(x + tw) - prefix(x).
+    // The window sum adds this row and drops the row th steps back (a ring of
+    // R >= th row sums; read before write when th == R).
     if (need_e) {
       constexpr int SE = S / 2;  // positions per energy thread
+      typedef Vec<RT, SE> VT;
       const int b = threadIdx.x - kEnergyWarp * 32;  // 0 .. 255
       const int tw = a.tw, th = a.th;  // registers: the item lives in shared memory
+      const int nq = P - 1 + tw;       // squares the windows cover
+      const int nqp = nq + 2 * SE;     // plus the zero pad the last loads read
+      const int nchunk = (tw + 2 * SE - 1) / SE;  // vector loads per thread and row
+      const int cfast = tw / SE;       // chunks 1 .. cfast - 1 lie inside every window
       ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
       ST* estage = reinterpret_cast<ST*>(smem + L.es);
+      RT* sqbuf = reinterpret_cast<RT*>(smem + L.sq);
+      const RT* mine = sqbuf + SE * b;
       WT ewin[SE];
 #pragma unroll
-      for (int p = 0; p < SE; ++p) ewin[p] = WT(0);
+      for (int i = 0; i < SE; ++i) ewin[i] = WT(0);
       int st = 0;
       uint32_t rph = 0;
       for (int t = 0; t < nsteps; ++t) {
@@ -591,33 +634,55 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
         // Ring entry ei was read by the epilogue (step t - kNE).
         ok = ok && (t < kNE || mbar_wait(&e_free[ei], ((t / kNE) - 1) & 1, abort_flag, kSpinLimit));
-        if (!__all_sync(0xffffffffu, ok)) break;
+        // The energy warps meet at named barriers: all take the same branch.
+        // This barrier also orders the previous row's reads of the squares
+        // before this row's writes.
+        uint32_t all;
+        asm volatile(
+            "{\n\t.reg .pred pi, po;\n\t"
+            "setp.ne.u32 pi, %1, 0;\n\t"
+            "barrier.red.and.pred po, %2, %3, pi;\n\t"
+            "selp.u32 %0, 1, 0, po;\n\t}"
+            : "=r"(all)
+            : "r"((uint32_t)ok), "n"(kBarEnergy), "n"(kEnergyThreads)
+            : "memory");
+        if (!all) break;
         const unsigned char* row = smem + L.raw + st * L.raw_stage;
+        for (int k = b; k < nqp; k += kEnergyThreads)
+          sqbuf[k] = k < nq ? sq_at<ELEM>(row, lead + k) : RT(0);
+        energy_sync();
+        // Prefix over the thread's V_0 .. : lo[i] = prefix(i), hi[i] = prefix(tw + i).
+        RT run = RT(0), lo[SE], hi[SE];
+        auto take = [&](const VT& v, int k0) {
+#pragma unroll
+          for (int j = 0; j < SE; ++j) {
+            const int k = k0 + j;
+#pragma unroll
+            for (int i = 0; i < SE; ++i) {  // static indices: lo and hi stay in registers
+              if (k == i) lo[i] = run;
+              if (k == tw + i) hi[i] = run;
+            }
+            run += v.v[j];
+          }
+        };
+        take(load_vec<RT, SE>(mine), 0);
+        int c = 1;
+        for (; c < cfast; ++c) {
+          const VT v = load_vec<RT, SE>(mine + SE * c);
+#pragma unroll
+          for (int j = 0; j < SE; ++j) run += v.v[j];
+        }
+        for (; c < nchunk; ++c) take(load_vec<RT, SE>(mine + SE * c), SE * c);
         ST* es = estage + ei * P;
-        RT rs[SE];
 #pragma unroll
-        for (int p = 0; p < SE; ++p) rs[p] = RT(0);
-        const int e0 = lead + b;
-        int w = 0;
-        for (; w + 8 <= tw; w += 8) {
-#pragma unroll
-          for (int d = 0; d < 8; ++d)
-#pragma unroll
-            for (int p = 0; p < SE; ++p) rs[p] += sq_at<ELEM>(row, e0 + kEnergyThreads * p + w + d);
-        }
-        for (; w < tw; ++w) {
-#pragma unroll
-          for (int p = 0; p < SE; ++p) rs[p] += sq_at<ELEM>(row, e0 + kEnergyThreads * p + w);
-        }
-#pragma unroll
-        for (int p = 0; p < SE; ++p) {
-          const int x = b + kEnergyThreads * p;
+        for (int i = 0; i < SE; ++i) {
+          const int x = SE * b + i;
           ST* slot = rsring + (t & (R - 1)) * P + x;
           const ST old = t >= th ? rsring[((t - th) & (R - 1)) * P + x] : ST(0);
-          const ST cur = static_cast<ST>(rs[p]);
+          const ST cur = static_cast<ST>(hi[i] - lo[i]);
           *slot = cur;
-          ewin[p] += static_cast<WT>(cur) - static_cast<WT>(old);
-          es[x] = static_cast<ST>(ewin[p]);
+          ewin[i] += static_cast<WT>(cur) - static_cast<WT>(old);
+          es[x] = static_cast<ST>(ewin[i]);
         }
         __syncwarp();
         if (lane == 0) {
