@@ -312,6 +312,34 @@ def test_tall_bands_many_blocks(ocip, ctx, dtype, th, tw, nch):
         ctx.set_path(ocip.PATH_PLAIN)
 
 
+def test_band_height_does_not_change_results(ocip, ctx):
+    """Items of 17, 64 or 150 rows, or the whole image, give the automatic
+    choice's maps: bit-identical for U8 (exact sums), within the 1e-5 bar for
+    F32 (the blocks of partial sums start at each band's first row). A negative
+    height is refused."""
+    ctx.make_current()
+    rng = np.random.default_rng(23)
+    S8 = rng.integers(0, 256, (300, 280), dtype=np.uint8)
+    T8 = rng.integers(0, 256, (20, 23), dtype=np.uint8)
+    Sf = rng.random((300, 280)).astype(np.float32)
+    Tf = rng.random((20, 23)).astype(np.float32)
+    try:
+        ref8 = {m: run(ocip, ctx, m, S8, T8, ocip.PATH_TENSOR)[0] for m in (0, 3)}
+        for rows in (17, 64, 150, 300):
+            ctx.set_band_height(rows)
+            for m in (0, 3):
+                got, path = run(ocip, ctx, m, S8, T8, ocip.PATH_TENSOR)
+                assert path == ocip.PATH_TENSOR
+                assert np.array_equal(got, ref8[m]), (MEAS[m], rows)
+            for m in (1, 4):
+                got, _ = run(ocip, ctx, m, Sf, Tf, ocip.PATH_TENSOR)
+                f32_check(got, Sf, Tf, m)
+        assert ocip.lib.ocipSetProximityBandHeight(-1) == ocip.CL_INVALID_VALUE
+    finally:
+        ctx.set_band_height(0)
+        ctx.set_path(ocip.PATH_PLAIN)
+
+
 def test_bounded_wait_expires_and_context_stays_usable(ocip, ctx):
     """A kernel waits on a barrier nothing arrives on: the bounded wait
     expires (about 1 ms here), the kernel returns, the error surfaces as
