@@ -231,9 +231,9 @@ __host__ __device__ inline Layout make_layout(bool split, const Geo& g, int nbox
   L.rs = L.a + kNA * L.a_stage;
   L.es = L.rs + g.R * g.P * 4;
   L.sq = L.es + g.kNE * g.P * 4;
-  // Squares of one staged row (8-byte entries at most), padded for the
+  // Squares of two staged rows (8-byte entries at most), each padded for the
   // energy threads' last vector loads.
-  L.bars = L.sq + align128((g.P + 64 + 32) * 8);
+  L.bars = L.sq + 2 * align128((g.P + 64 + 32) * 8);
   // raw full, raw free; ready, MMA done; energy full, energy free (16 each
   // at most); block full, buffer free; done.
   L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNA + 32 + 4 + 1));
@@ -605,12 +605,13 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     }
   } else if (warp >= kEnergyWarp) {
     // ---- Window energies ----------------------------------------------------------
-    // Per staged row the squares V_k = S^2(lead + k) are written once to a
+    // Two staged rows per pass (their chains interleave; one barrier pair per
+    // two rows). Per row the squares V_k = S^2(lead + k) are written once to a
     // buffer; thread b then takes the SE = S / 2 consecutive positions
     // x = SE b + i and streams V_{SE b} .. with aligned vector loads, keeping a
     // running prefix: the row sum of position x is prefix(x + tw) - prefix(x).
-    // The window sum adds this row and drops the row th steps back (a ring of
-    // R >= th row sums; read before write when th == R).
+    // The window sum adds each row and drops the row th steps back (a ring of
+    // R >= th row sums; read before write when th == R), in row order.
     if (need_e) {
       constexpr int SE = S / 2;  // positions per energy thread
       typedef Vec<RT, SE> VT;
@@ -620,23 +621,31 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
       const int nqp = nq + 2 * SE;     // plus the zero pad the last loads read
       const int nchunk = (tw + 2 * SE - 1) / SE;  // vector loads per thread and row
       const int cfast = tw / SE;       // chunks 1 .. cfast - 1 lie inside every window
+      const int sqstride = align128((P + 64 + 32) * 8) / (int)sizeof(RT);  // RT per buffer
       ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
       ST* estage = reinterpret_cast<ST*>(smem + L.es);
       RT* sqbuf = reinterpret_cast<RT*>(smem + L.sq);
-      const RT* mine = sqbuf + SE * b;
       WT ewin[SE];
 #pragma unroll
       for (int i = 0; i < SE; ++i) ewin[i] = WT(0);
       int st = 0;
       uint32_t rph = 0;
-      for (int t = 0; t < nsteps; ++t) {
-        const int ei = t % kNE;
+      for (int t = 0; t < nsteps; t += 2) {
+        const bool two = t + 1 < nsteps;  // uniform
+        const int st1 = st + 1 == kNRaw ? 0 : st + 1;
+        const uint32_t rph1 = st + 1 == kNRaw ? rph ^ 1 : rph;
         bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
-        // Ring entry ei was read by the epilogue (step t - kNE).
-        ok = ok && (t < kNE || mbar_wait(&e_free[ei], ((t / kNE) - 1) & 1, abort_flag, kSpinLimit));
+        // Ring entries of rows t, t + 1 were read by the epilogue (kNE rows back).
+        ok = ok && (t < kNE ||
+                    mbar_wait(&e_free[t % kNE], ((t / kNE) - 1) & 1, abort_flag, kSpinLimit));
+        if (two) {
+          ok = ok && mbar_wait(&raw_full[st1], rph1, abort_flag, kSpinLimit);
+          ok = ok && (t + 1 < kNE || mbar_wait(&e_free[(t + 1) % kNE], (((t + 1) / kNE) - 1) & 1,
+                                               abort_flag, kSpinLimit));
+        }
         // The energy warps meet at named barriers: all take the same branch.
-        // This barrier also orders the previous row's reads of the squares
-        // before this row's writes.
+        // This barrier also orders the previous pass's reads of the squares
+        // before this pass's writes.
         uint32_t all;
         asm volatile(
             "{\n\t.reg .pred pi, po;\n\t"
@@ -647,49 +656,75 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
             : "r"((uint32_t)ok), "n"(kBarEnergy), "n"(kEnergyThreads)
             : "memory");
         if (!all) break;
-        const unsigned char* row = smem + L.raw + st * L.raw_stage;
-        for (int k = b; k < nqp; k += kEnergyThreads)
-          sqbuf[k] = k < nq ? sq_at<ELEM>(row, lead + k) : RT(0);
+        const unsigned char* row0 = smem + L.raw + st * L.raw_stage;
+        const unsigned char* row1 = smem + L.raw + st1 * L.raw_stage;
+        for (int k = b; k < nqp; k += kEnergyThreads) {
+          sqbuf[k] = k < nq ? sq_at<ELEM>(row0, lead + k) : RT(0);
+          if (two) sqbuf[sqstride + k] = k < nq ? sq_at<ELEM>(row1, lead + k) : RT(0);
+        }
         energy_sync();
-        // Prefix over the thread's V_0 .. : lo[i] = prefix(i), hi[i] = prefix(tw + i).
-        RT run = RT(0), lo[SE], hi[SE];
-        auto take = [&](const VT& v, int k0) {
+        // Prefixes over the thread's V_0 ..: lo[r][i] = prefix(i), hi[r][i] = prefix(tw + i).
+        const RT* m0 = sqbuf + SE * b;
+        const RT* m1 = m0 + sqstride;
+        RT run[2] = {RT(0), RT(0)}, lo[2][SE], hi[2][SE];
+        auto take = [&](const VT& v0, const VT& v1, int k0) {
 #pragma unroll
           for (int j = 0; j < SE; ++j) {
             const int k = k0 + j;
 #pragma unroll
             for (int i = 0; i < SE; ++i) {  // static indices: lo and hi stay in registers
-              if (k == i) lo[i] = run;
-              if (k == tw + i) hi[i] = run;
+              if (k == i) {
+                lo[0][i] = run[0];
+                lo[1][i] = run[1];
+              }
+              if (k == tw + i) {
+                hi[0][i] = run[0];
+                hi[1][i] = run[1];
+              }
             }
-            run += v.v[j];
+            run[0] += v0.v[j];
+            run[1] += v1.v[j];
           }
         };
-        take(load_vec<RT, SE>(mine), 0);
+        take(load_vec<RT, SE>(m0), load_vec<RT, SE>(m1), 0);
         int c = 1;
         for (; c < cfast; ++c) {
-          const VT v = load_vec<RT, SE>(mine + SE * c);
+          const VT v0 = load_vec<RT, SE>(m0 + SE * c);
+          const VT v1 = load_vec<RT, SE>(m1 + SE * c);
 #pragma unroll
-          for (int j = 0; j < SE; ++j) run += v.v[j];
+          for (int j = 0; j < SE; ++j) {
+            run[0] += v0.v[j];
+            run[1] += v1.v[j];
+          }
         }
-        for (; c < nchunk; ++c) take(load_vec<RT, SE>(mine + SE * c), SE * c);
-        ST* es = estage + ei * P;
+        for (; c < nchunk; ++c) take(load_vec<RT, SE>(m0 + SE * c), load_vec<RT, SE>(m1 + SE * c), SE * c);
 #pragma unroll
-        for (int i = 0; i < SE; ++i) {
-          const int x = SE * b + i;
-          ST* slot = rsring + (t & (R - 1)) * P + x;
-          const ST old = t >= th ? rsring[((t - th) & (R - 1)) * P + x] : ST(0);
-          const ST cur = static_cast<ST>(hi[i] - lo[i]);
-          *slot = cur;
-          ewin[i] += static_cast<WT>(cur) - static_cast<WT>(old);
-          es[x] = static_cast<ST>(ewin[i]);
+        for (int r = 0; r < 2; ++r) {
+          if (r == 1 && !two) break;
+          const int tr = t + r;
+          ST* es = estage + (tr % kNE) * P;
+#pragma unroll
+          for (int i = 0; i < SE; ++i) {
+            const int x = SE * b + i;
+            ST* slot = rsring + (tr & (R - 1)) * P + x;
+            const ST old = tr >= th ? rsring[((tr - th) & (R - 1)) * P + x] : ST(0);
+            const ST cur = static_cast<ST>(hi[r][i] - lo[r][i]);
+            *slot = cur;
+            ewin[i] += static_cast<WT>(cur) - static_cast<WT>(old);
+            es[x] = static_cast<ST>(ewin[i]);
+          }
         }
         __syncwarp();
         if (lane == 0) {
-          mbar_arrive(&e_full[ei]);
+          mbar_arrive(&e_full[t % kNE]);
           mbar_arrive(&raw_free[st]);
+          if (two) {
+            mbar_arrive(&e_full[(t + 1) % kNE]);
+            mbar_arrive(&raw_free[st1]);
+          }
         }
-        if (++st == kNRaw) { st = 0; rph ^= 1; }
+        st = two ? (st1 + 1 == kNRaw ? 0 : st1 + 1) : st1;
+        rph = two ? (st1 + 1 == kNRaw ? rph1 ^ 1 : rph1) : rph1;
       }
     }
   } else {
