@@ -142,13 +142,25 @@ def dist_setup():
 
 
 def allreduce_max(x):
+    """Max of x over the ranks (x on every rank when not distributed). The
+    tensor lives where the backend wants it: GPU for NCCL, host for gloo."""
     import torch
     import torch.distributed as dist
     if not dist.is_initialized():
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard(items, rank, world):
+    """This rank's share of independent work items (images of a batch):
+    every world-th item from `rank`. The shares are disjoint, cover the list
+    and differ in size by at most one; the path needs no exchange between
+    ranks."""
+    items = list(items)
+    return items[rank::world] if world > 1 else items
 
 
 def barrier():
@@ -458,7 +470,7 @@ def run_batch_bench(args, world, rank, local):
     from openclipp_b200 import ocip
 
     imgs, tmpls = batch_workload()
-    mine = imgs[rank::world] if world > 1 else imgs
+    mine = shard(imgs, rank, world)
     side = imgs[0].shape[0]
     taps_meas = sum(len(mine) * (side - t.shape[0] + 1) ** 2 * t.size for t in tmpls)
     measures = ["CrossCorr", "SqrDistance"]
