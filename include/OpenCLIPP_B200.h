@@ -90,7 +90,7 @@ enum ocipMeasure {
  * (1-4); templates are at most 64 x 64 and no larger than any image; each
  * Dest is F32 or F64 with its image's size and channels. AbsDistance has no
  * tensor-core form and is refused (CL_INVALID_VALUE). The work is a queue of
- * (pair, channel, 256-column strip, band of rows) items, largest first,
+ * (pair, channel, column strip, band of rows) items, largest first,
  * taken by one persistent CTA per SM on the tensor path (U8 exact; F32 and
  * U16 within 1e-5 relative). Band heights are chosen per (template size
  * class, type, channels) by timing candidates on the device the first time a
