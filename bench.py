@@ -676,6 +676,136 @@ def run_backward_bench(args, world, rank, local):
     }
 
 
+def run_integral_bench(args, world, rank, local):
+    """Integral scan workload: Integral and SqrIntegral of the 4096x4096 F32
+    blob field into F64 tables, one of each per step. Algorithmic bytes per
+    table: the source read once (4 B/px) and the table written once (8 B/px).
+    The tables are checked against the exact integral of the oracle."""
+    import torch
+
+    from openclipp_b200 import ocip
+    from oracle import oracle as O
+
+    S = workload(seed=1234 + rank)[0]
+    H, W = S.shape
+    ctx = ocip.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    Si = ocip.Image(S)
+    outs = [np.zeros((H, W), np.float64) for _ in range(2)]
+    Ds = [ocip.Image(o) for o in outs]
+    Si.send()
+    prog = ocip.prepare_integral(Si)
+    per_table = {0: [], 1: []}
+
+    def timed(n, record=False):
+        times = []
+        for _ in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(stream)
+            for sqr in (0, 1):
+                ocip.integral(prog, Si, Ds[sqr], sqr=bool(sqr))
+                ev[sqr + 1].record(stream)
+            ev[2].synchronize()
+            times.append(ev[0].elapsed_time(ev[2]))
+            if record:
+                for sqr in (0, 1):
+                    per_table[sqr].append(ev[sqr].elapsed_time(ev[sqr + 1]))
+        return times
+
+    timed(args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    # A step is ~0.15 ms: at least 2000 steps so that the clock sampler
+    # (100 ms period) sees the timed region.
+    steps = max(args.steps, 2000)
+    launches0 = ocip.launch_count()
+    with Clocks(local) as clk:
+        times = timed(steps, record=True)
+    launches = ocip.launch_count() - launches0
+    ms_step = allreduce_max(float(np.mean(times)))
+
+    exact = True
+    if rank == 0:
+        for sqr in (0, 1):
+            Ds[sqr].read()
+            ex = O.integral_exact(S, sqr)
+            rel = float(np.abs(outs[sqr] - ex).max() / np.abs(ex).max())
+            exact = exact and rel < 1e-12
+
+    # End-to-end: pinned host source in, both tables out, every step.
+    hS = torch.empty((H, W), dtype=torch.float32, pin_memory=True).numpy()
+    hS[:] = S
+    houts = [torch.empty((H, W), dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    hSi = ocip.Image(hS)
+    hDs = [ocip.Image(o) for o in houts]
+
+    def e2e_step():
+        hSi.send()
+        for sqr in (0, 1):
+            ocip.integral(prog, hSi, hDs[sqr], sqr=bool(sqr))
+        for D in hDs:
+            D.read()
+
+    for _ in range(3):
+        e2e_step()
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 5))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_t.append(e0.elapsed_time(e1))
+    e2e_ms = allreduce_max(float(np.mean(e2e_t)))
+
+    bytes_table = W * H * (4 + 8)
+    bytes_step = 2 * bytes_table
+    peaks = load_peaks()
+    med = {k: float(np.median(v)) for k, v in per_table.items()}
+    dom = max(med, key=med.get)
+    gbs = bytes_table / (med[dom] * 1e-3) / 1e9
+    result = {
+        "metric": "integral table throughput (Integral + SqrIntegral, F32 -> F64)",
+        "value": round(bytes_step * world / (ms_step * 1e-3) / 1e9, 1), "unit": "GB/s",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded blob field)",
+        "config": {"workload": f"{W}x{H} F32 1ch -> F64 Integral and SqrIntegral per step",
+                   "bytes_per_step": bytes_step,
+                   "bytes_counted": "source read once + table written once, per table",
+                   "l2": "flushed before every step (256 MiB write, outside the timed events)"},
+        "per_table_ms": {"Integral": round(med[0], 4), "SqrIntegral": round(med[1], 4)},
+        "exact_vs_oracle": exact,
+        "roofline": {"kernel": ["Integral", "SqrIntegral"][dom] + " (3 launches)",
+                     "bound": "hbm", "achieved": round(gbs, 1), "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": round(gbs / peaks["hbm_gbs"], 4),
+                     "traffic": None, "peak_source": peaks["source"]},
+        "e2e": {"value": round(bytes_step * world / (e2e_ms * 1e-3) / 1e9, 1), "unit": "GB/s",
+                "h2d_bytes_per_step": int(S.nbytes),
+                "d2h_bytes_per_step": int(sum(o.nbytes for o in houts))},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline and O.ref_available():
+        rows = 512
+        t0 = time.perf_counter()
+        for sqr in (0, 1):
+            O.integral_reference(np.ascontiguousarray(S[:rows]), sqr, True)
+        dt = time.perf_counter() - t0
+        result["cpu_baseline"] = {
+            "value": round(2 * rows * W * 12 / dt / 1e9, 3), "unit": "GB/s", "cores": 1,
+            "kind": "reference",
+            "sample": f"rows 0-{rows} of the {W}x{H} source, Integral + SqrIntegral, "
+                      f"cl-files/Integral.cl pipeline built for the host, {dt:.2f} s"}
+    for D in Ds + hDs + [Si, hSi, prog]:
+        D.release()
+    ctx.close()
+    return result
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -688,10 +818,12 @@ def main():
     ap.add_argument("--measures", default=",".join(MEASURES),
                     help="comma-separated subset of the five measures (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm (profiling)")
-    ap.add_argument("--workload", choices=["single", "batch", "backward"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "backward", "integral"],
+                    default="single",
                     help="single: 4096^2 F32, 31x31, five measures (the headline); batch: 16 x "
                          "2048^2 U8 x 64 uneven templates in persistent launches; backward: "
-                         "32 x 1024^2 F32 with 32x32 templates, gradients vs forward time")
+                         "32 x 1024^2 F32 with 32x32 templates, gradients vs forward time; "
+                         "integral: 4096^2 F32 Integral + SqrIntegral into F64 tables")
     args = ap.parse_args()
     args.measures = [m for m in args.measures.split(",") if m]
     assert all(m in MEASURES for m in args.measures), args.measures
@@ -708,6 +840,8 @@ def main():
         res = run_batch_bench(args, world, rank, local)
     elif args.workload == "backward":
         res = run_backward_bench(args, world, rank, local)
+    elif args.workload == "integral":
+        res = run_integral_bench(args, world, rank, local)
     else:
         res = run_ours(args, world, rank, local)
     if rank == 0:

@@ -10,29 +10,40 @@
 // the destination type (its F32 result is exact only while sums stay below
 // 2^24).
 //
-// Layout: the image is cut into 256 x 64 tiles, one warp per tile (lane l
-// holds 8 consecutive columns). Three passes, each reading the source once
-// with coalesced loads (the second read mostly hits L2):
-//   1. tile reduce: per-row tile sums (RowSum) and the tile-local column
-//      prefix of the tile's column sums (LB) -- the counterpart of the
-//      reference's vertical/horizontal junction buffers;
-//   2. junctions: RowLeft = exclusive scan of RowSum across tiles of a row,
-//      BandLeft = exclusive scan of tile totals across a band, Top = exclusive
-//      scan over bands of (BandLeft + LB) per column (the full integral of the
-//      row just above each band);
-//   3. final: D = Top + running sum over the band's rows of
-//      (RowLeft + warp-scanned row prefix), one store per pixel.
+// Layout: the image is cut into 128 x 32 tiles, one warp per tile (lane l
+// holds 4 consecutive columns, so one vector load of a warp reads 128
+// contiguous pixels when the image allows it). A warp loads a group of 8 rows
+// (4 for 8-byte types) before it sums any of them, and the kernels stay
+// within 64 registers so that 32 warps share an SM: a 4096 x 4096 image is
+// 4096 tiles, all resident at once on 148 SMs. Three launches:
+//   1. tile reduce (reads the source): per-row tile sums (RowSum), the tile's
+//      local integral at its bottom row (LB) and the tile's total (TT) -- the
+//      counterpart of the reference's vertical/horizontal junction buffers;
+//   2. junctions, one launch with two kinds of blocks: a warp per row turns
+//      RowSum into RowLeft (exclusive scan across the tiles of the row), and
+//      blocks of 32 columns turn LB into Top (exclusive scan over bands of
+//      BandLeft + LB, BandLeft = the band's tile totals left of the column's
+//      tile), which is the full integral of the row just above each band;
+//   3. final (reads the source again, mostly from L2): D = Top + running sum
+//      over the band's rows of (RowLeft + warp-scanned row prefix).
 #include <cuda_runtime.h>
+
+#include <cstring>
 
 #include "internal.h"
 
 namespace ocipb {
 namespace {
 
-constexpr int kTW = 256;   // tile width (32 lanes x 8 columns)
-constexpr int kTH = 64;    // tile height
-constexpr int kPX = 8;     // columns per lane
+constexpr int kTW = 128;   // tile width (32 lanes x 4 columns)
+constexpr int kTH = 32;    // tile height
+constexpr int kPX = 4;     // columns per lane
 constexpr int kWarpsPerCta = 4;
+constexpr int kMinCtas = 8;      // 32 warps per SM: at most 64 registers
+constexpr int kJThreads = 256;   // junction blocks
+constexpr int kJCols = 32;       // columns per Top block
+constexpr int kJBands = 16;      // bands per thread and chunk step in a Top block
+constexpr int kJRows = 8;        // image rows per warp in a RowLeft block
 
 template <int TYPE> struct ElemOf;
 template <> struct ElemOf<U8> { typedef uint8_t T; };
@@ -52,9 +63,11 @@ struct IntegralParams {
   int dst_f64;
   int W, H, nch;
   int nBX, nBY;
+  int vec_src;     // 1: one channel, 16-byte aligned base and pitch
+  int vec_dst;     // 1: one channel, base and pitch aligned to a lane's 4 pixels
   void* rowsum;    // [nch][H][nBX]     RowSum, then RowLeft
   void* lb;        // [nch][nBY][W]     LB, then Top
-  void* bandleft;  // [nch][nBY][nBX]
+  void* tt;        // [nch][nBY][nBX]   tile totals
 };
 
 template <typename A>
@@ -67,31 +80,211 @@ __device__ __forceinline__ A warp_incl_scan(A v, int lane) {
   return v;
 }
 
-template <typename A>
-__device__ __forceinline__ A warp_sum(A v) {
+// Totals of G rows across the warp with G - 1 + log2(32 / G) shuffles instead
+// of 5 G: at each halving step a lane keeps the half of its rows selected by
+// its lane bit and adds the partner's copy of them. On return every lane
+// holds the total of row (lane >> (5 - log2 G)). G is a power of two <= 32.
+template <int G, typename A>
+__device__ __forceinline__ A warp_sum_rows(A (&s)[G], int lane) {
 #pragma unroll
-  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  for (int lvl = 0; (G >> lvl) > 1; ++lvl) {
+    const int o = 16 >> lvl;
+    constexpr int kMax = G / 2;
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < kMax; ++i) {
+      if (i < (G >> lvl) / 2) {
+        const int h = (G >> lvl) / 2;
+        const A send = upper ? s[i] : s[i + h];
+        const A keep = upper ? s[i + h] : s[i];
+        s[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+  }
+  A v = s[0];
+#pragma unroll
+  for (int o = 16 / G; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
-// Loads the lane's 8 values of row y (zero outside the image), squared if SQR.
-template <int TYPE, typename A, bool SQR>
-__device__ __forceinline__ void load_row(const IntegralParams& p, int c, int y,
-                                         int xl, A (&v)[kPX]) {
-  using ET = typename ElemOf<TYPE>::T;
-  const ET* row = reinterpret_cast<const ET*>(p.src + (size_t)y * p.src_pitch);
+template <int G>
+__host__ __device__ constexpr int log2_of() { return G <= 1 ? 0 : 1 + log2_of<G / 2>(); }
+
+// Rows a warp loads before it consumes any: 4 KB per warp for 4-byte types.
+template <typename ET>
+__host__ __device__ constexpr int group_rows() { return sizeof(ET) >= 8 ? 4 : 8; }
+
+// The lane's 4 source values of a row, as one vector load (two for 8-byte
+// types): the row is 16-byte aligned and the 4 columns are inside the image.
+template <typename ET>
+__device__ __forceinline__ void load_vec(const ET* row, int xl, ET (&e)[kPX]) {
+  if constexpr (sizeof(ET) == 1) {
+    const uint32_t q = *reinterpret_cast<const uint32_t*>(row + xl);
+    memcpy(e, &q, sizeof(q));
+  } else if constexpr (sizeof(ET) == 2) {
+    const uint2 q = *reinterpret_cast<const uint2*>(row + xl);
+    memcpy(e, &q, sizeof(q));
+  } else {
+    constexpr int NQ = sizeof(ET) * kPX / 16;
+    uint4 q[NQ];
 #pragma unroll
-  for (int k = 0; k < kPX; ++k) {
-    const int x = xl + k;
-    A a = A(0);
-    if (x < p.W) a = (A)row[(size_t)x * p.nch + c];
-    v[k] = SQR ? a * a : a;
+    for (int i = 0; i < NQ; ++i) q[i] = reinterpret_cast<const uint4*>(row + xl)[i];
+    memcpy(e, q, sizeof(q));
   }
 }
 
+// The lane's 4 source values of row y, zero outside the image.
+template <typename ET>
+__device__ __forceinline__ void load_raw(const IntegralParams& p, int c, int y, int xl,
+                                         ET (&e)[kPX]) {
+  const ET* row = reinterpret_cast<const ET*>(p.src + (size_t)y * p.src_pitch);
+  if (p.vec_src && xl + kPX <= p.W) {
+    load_vec(row, xl, e);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < kPX; ++k) {
+    const int x = xl + k;
+    e[k] = x < p.W ? row[(size_t)x * p.nch + c] : ET(0);
+  }
+}
+
+// Rows yg .. yg + G - 1 of the lane's columns (zero from row yend on). When
+// the whole group lies inside the image and the tile's columns are vector
+// loadable (both warp-uniform), the G loads are issued back to back.
+template <int G, typename ET>
+__device__ __forceinline__ void load_group(const IntegralParams& p, int c, int yg, int yend,
+                                           int xl, bool vec_tile, ET (&raw)[G][kPX]) {
+  if (vec_tile && yg + G <= yend) {
+    const char* base = p.src + (size_t)yg * p.src_pitch;
+#pragma unroll
+    for (int r = 0; r < G; ++r)
+      load_vec(reinterpret_cast<const ET*>(base + (size_t)r * p.src_pitch), xl, raw[r]);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < G; ++r) {
+    if (yg + r < yend) {
+      load_raw(p, c, yg + r, xl, raw[r]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kPX; ++k) raw[r][k] = ET(0);
+    }
+  }
+}
+
+template <typename A, bool SQR, typename ET>
+__device__ __forceinline__ A value_of(ET e) {
+  const A a = (A)e;
+  return SQR ? a * a : a;
+}
+
+// ---- Per-lane row stream through shared memory ------------------------------
+//
+// On the vector path each lane copies its own kPX pixels of every tile row
+// into a ring of kDepth slots with cp.async, kDepth rows ahead of the row it
+// consumes, and reads back only what it copied itself, so no lane waits for
+// another. The copies in flight hold no registers: a warp keeps kDepth rows
+// (4 KB for 4-byte pixels) in flight whatever its per-row work.
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "n"(BYTES)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <typename ET>
+struct RowStream {
+  static constexpr int kLane = kPX * (int)sizeof(ET);  // bytes per lane and row
+  static constexpr int kDepth = kLane > 16 ? 4 : 8;
+  static constexpr int kSlot = 32 * kLane;             // one warp-row
+  static constexpr int kWarpBytes = kDepth * kSlot;
+
+  unsigned char* mine;  // this lane's bytes in slot 0
+  const char* src;      // this lane's pixels in row 0 of the tile
+  size_t pitch;
+  int nrows;
+
+  __device__ __forceinline__ RowStream(unsigned char* warp_ring, int lane, const char* row0,
+                                       size_t pitch_, int nrows_)
+      : mine(warp_ring + lane * kLane), src(row0), pitch(pitch_), nrows(nrows_) {}
+
+  __device__ __forceinline__ void copy(int y) const {
+    unsigned char* d = mine + (y & (kDepth - 1)) * kSlot;
+    const char* g = src + (size_t)y * pitch;
+    if constexpr (kLane <= 16) {
+      cp_async<kLane>(d, g);
+    } else {
+      cp_async<16>(d, g);
+      cp_async<16>(d + 16, g + 16);
+    }
+  }
+
+  // Rows 0 .. kDepth - 1 in flight; one commit group per row, empty past the
+  // tile's last row, so that group y always holds row y.
+  __device__ __forceinline__ void start() const {
+#pragma unroll
+    for (int d = 0; d < kDepth; ++d) {
+      if (d < nrows) copy(d);
+      cp_async_commit();
+    }
+  }
+
+  // Row y (y < nrows) once its group has landed.
+  __device__ __forceinline__ void read(int y, ET (&e)[kPX]) const {
+    cp_async_wait<kDepth - 1>();
+    const unsigned char* d = mine + (y & (kDepth - 1)) * kSlot;
+    if constexpr (kLane == 4) {
+      const uint32_t q = *reinterpret_cast<const uint32_t*>(d);
+      memcpy(e, &q, sizeof(q));
+    } else if constexpr (kLane == 8) {
+      const uint2 q = *reinterpret_cast<const uint2*>(d);
+      memcpy(e, &q, sizeof(q));
+    } else if constexpr (kLane == 16) {
+      const uint4 q = *reinterpret_cast<const uint4*>(d);
+      memcpy(e, &q, sizeof(q));
+    } else {
+      uint4 q[2];
+      q[0] = reinterpret_cast<const uint4*>(d)[0];
+      q[1] = reinterpret_cast<const uint4*>(d)[1];
+      memcpy(e, q, sizeof(q));
+    }
+  }
+
+  // Reuse row y's slot for row y + kDepth. The warp barrier orders the read
+  // of the slot before the copy that overwrites it.
+  __device__ __forceinline__ void refill(int y) const {
+    __syncwarp();
+    if (y + kDepth < nrows) copy(y + kDepth);
+    cp_async_commit();
+  }
+
+  __device__ __forceinline__ void drain() const { cp_async_wait<0>(); }
+};
+
 template <int TYPE, typename A, bool SQR>
-__global__ void __launch_bounds__(32 * kWarpsPerCta)
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
     integral_reduce_kernel(const IntegralParams p) {
+  using ET = typename ElemOf<TYPE>::T;
+  constexpr int G = group_rows<ET>();
   const int lane = threadIdx.x & 31;
   const int tile = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
   const int c = blockIdx.y;
@@ -101,24 +294,68 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   const int y0 = by * kTH;
   A* rowsum = reinterpret_cast<A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
   A* lb = reinterpret_cast<A*>(p.lb) + (size_t)c * p.nBY * p.W;
+  A* tt = reinterpret_cast<A*>(p.tt) + (size_t)c * p.nBY * p.nBX;
   A col[kPX];
 #pragma unroll
   for (int k = 0; k < kPX; ++k) col[k] = A(0);
   const int yend = min(p.H, y0 + kTH);
-  for (int y = y0; y < yend; ++y) {
-    A v[kPX];
-    load_row<TYPE, A, SQR>(p, c, y, xl, v);
-    A s = A(0);
+  const bool vec_tile = p.vec_src && (bx + 1) * kTW <= p.W;
+  if (vec_tile) {
+    using RS = RowStream<ET>;
+    __shared__ __align__(16) unsigned char ring[kWarpsPerCta * RS::kWarpBytes];
+    const int nrows = yend - y0;
+    const RS rs(ring + (threadIdx.x >> 5) * RS::kWarpBytes, lane,
+                p.src + (size_t)y0 * p.src_pitch + (size_t)xl * sizeof(ET), p.src_pitch, nrows);
+    rs.start();
+    for (int yg = 0; yg < nrows; yg += G) {
+      A s[G];
 #pragma unroll
-    for (int k = 0; k < kPX; ++k) {
-      s += v[k];
-      col[k] += v[k];
+      for (int r = 0; r < G; ++r) {
+        s[r] = A(0);
+        if (yg + r < nrows) {
+          ET e[kPX];
+          rs.read(yg + r, e);
+#pragma unroll
+          for (int k = 0; k < kPX; ++k) {
+            const A v = value_of<A, SQR>(e[k]);
+            s[r] += v;
+            col[k] += v;
+          }
+          rs.refill(yg + r);
+        }
+      }
+      const A tot = warp_sum_rows<G>(s, lane);
+      const int r = lane >> (5 - log2_of<G>());
+      if ((lane & (32 / G - 1)) == 0 && yg + r < nrows)
+        rowsum[(size_t)(y0 + yg + r) * p.nBX + bx] = tot;
     }
-    s = warp_sum(s);
-    if (lane == 0) rowsum[(size_t)y * p.nBX + bx] = s;
+    rs.drain();
+  } else {
+    // Generic layouts (several channels, unaligned rows, the image's right
+    // edge): register groups of rows.
+    constexpr int GG = G / 2;
+    for (int yg = y0; yg < yend; yg += GG) {
+      ET raw[GG][kPX];
+      load_group<GG>(p, c, yg, yend, xl, false, raw);
+      A s[GG];
+#pragma unroll
+      for (int r = 0; r < GG; ++r) {
+        s[r] = A(0);
+#pragma unroll
+        for (int k = 0; k < kPX; ++k) {
+          const A v = value_of<A, SQR>(raw[r][k]);
+          s[r] += v;
+          col[k] += v;
+        }
+      }
+      const A tot = warp_sum_rows<GG>(s, lane);
+      const int r = lane >> (5 - log2_of<GG>());
+      if ((lane & (32 / GG - 1)) == 0 && yg + r < yend)
+        rowsum[(size_t)(yg + r) * p.nBX + bx] = tot;
+    }
   }
   // Tile-local prefix of the column sums along x = the tile's local integral
-  // at its bottom row.
+  // at its bottom row; lane 31's inclusive value is the tile's total.
 #pragma unroll
   for (int k = 1; k < kPX; ++k) col[k] += col[k - 1];
   const A incl = warp_incl_scan(col[kPX - 1], lane);
@@ -126,49 +363,113 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
 #pragma unroll
   for (int k = 0; k < kPX; ++k)
     if (xl + k < p.W) lb[(size_t)by * p.W + xl + k] = excl + col[k];
+  if (lane == 31) tt[(size_t)by * p.nBX + bx] = incl;
 }
 
-// RowLeft (thread per row) and BandLeft (thread per band), both exclusive
-// scans across the tiles of a row / band.
+// Junctions. Blocks [0, top_blocks): kJCols columns each (inside one tile
+// column, since kJCols divides kTW), LB -> Top in place, bands taken in chunks
+// of 8 x kJBands: thread (column, group g) loads kJBands bands, the groups'
+// totals are combined through shared memory. These blocks have the longer
+// dependency chain, so they come first in the grid. Blocks after them: a
+// warp per kJRows image rows, RowSum -> RowLeft in place.
 template <typename A>
-__global__ void integral_junction_rows_kernel(const IntegralParams p) {
+__global__ void __launch_bounds__(kJThreads, 2)
+    integral_junction_kernel(const IntegralParams p, int top_blocks) {
+  constexpr int kGroups = kJThreads / kJCols;
+  constexpr int kChunk = kGroups * kJBands;
+  __shared__ A band_left[kChunk];
+  __shared__ A group_total[kGroups][kJCols];
   const int c = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  A* rowsum = reinterpret_cast<A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
-  const A* lb = reinterpret_cast<const A*>(p.lb) + (size_t)c * p.nBY * p.W;
-  A* bl = reinterpret_cast<A*>(p.bandleft) + (size_t)c * p.nBY * p.nBX;
-  if (i < p.H) {
-    A run = A(0);
-    for (int bx = 0; bx < p.nBX; ++bx) {
-      const A v = rowsum[(size_t)i * p.nBX + bx];
-      rowsum[(size_t)i * p.nBX + bx] = run;
-      run += v;
+  const int lane = threadIdx.x & 31;
+  // Launched as a programmatic dependent of the reduce launch: everything
+  // read here is written by it.
+  cudaGridDependencySynchronize();
+  if ((int)blockIdx.x >= top_blocks) {
+    // kJRows rows per warp, their loads issued together (clamped addresses).
+    const int y0 = ((blockIdx.x - top_blocks) * (kJThreads / 32) + (threadIdx.x >> 5)) * kJRows;
+    if (y0 >= p.H) return;
+    A* rs = reinterpret_cast<A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
+    A carry[kJRows];
+#pragma unroll
+    for (int i = 0; i < kJRows; ++i) carry[i] = A(0);
+    for (int b0 = 0; b0 < p.nBX; b0 += 32) {
+      const int b = b0 + lane;
+      A v[kJRows];
+#pragma unroll
+      for (int i = 0; i < kJRows; ++i)
+        v[i] = rs[(size_t)min(y0 + i, p.H - 1) * p.nBX + min(b, p.nBX - 1)];
+#pragma unroll
+      for (int i = 0; i < kJRows; ++i) {
+        if (b >= p.nBX) v[i] = A(0);
+        const A incl = warp_incl_scan(v[i], lane);
+        if (b < p.nBX && y0 + i < p.H) rs[(size_t)(y0 + i) * p.nBX + b] = carry[i] + (incl - v[i]);
+        carry[i] += __shfl_sync(0xffffffffu, incl, 31);
+      }
     }
-  } else if (i < p.H + p.nBY) {
-    const int by = i - p.H;
-    A run = A(0);
-    for (int bx = 0; bx < p.nBX; ++bx) {
-      bl[(size_t)by * p.nBX + bx] = run;
-      const int xe = min(p.W, (bx + 1) * kTW) - 1;
-      run += lb[(size_t)by * p.W + xe];
-    }
+    return;
   }
-}
-
-// Top[by][x] = sum over bands above of (BandLeft + LB), in place over LB.
-template <typename A>
-__global__ void integral_junction_cols_kernel(const IntegralParams p) {
-  const int c = blockIdx.y;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= p.W) return;
   A* lb = reinterpret_cast<A*>(p.lb) + (size_t)c * p.nBY * p.W;
-  const A* bl = reinterpret_cast<const A*>(p.bandleft) + (size_t)c * p.nBY * p.nBX;
-  const int bx = x / kTW;
-  A run = A(0);
-  for (int by = 0; by < p.nBY; ++by) {
-    const A v = bl[(size_t)by * p.nBX + bx] + lb[(size_t)by * p.W + x];
-    lb[(size_t)by * p.W + x] = run;
-    run += v;
+  const A* tt = reinterpret_cast<const A*>(p.tt) + (size_t)c * p.nBY * p.nBX;
+  const int x0 = blockIdx.x * kJCols;
+  const int x = x0 + lane;
+  const int g = threadIdx.x >> 5;
+  const int bx = x0 / kTW;
+  A carry = A(0);
+  for (int b0 = 0; b0 < p.nBY; b0 += kChunk) {
+    // This thread's LB values (column x, bands g * kJBands + j), issued first
+    // so that they are in flight while BandLeft is summed. Clamped (always
+    // valid) addresses, masked afterwards: a load whose use sits in the same
+    // branch would stall the warp before the next load issues.
+    A v[kJBands];
+    const int xc = min(x, p.W - 1);
+#pragma unroll
+    for (int j = 0; j < kJBands; ++j)
+      v[j] = lb[(size_t)min(b0 + g * kJBands + j, p.nBY - 1) * p.W + xc];
+    {
+      // BandLeft of the warp's bands g * kJBands .. + kJBands - 1: the tile
+      // totals left of this tile, lane j taking tile columns j, j + 32, ...;
+      // one multi-row warp reduction combines them. Only warp g reads them.
+      A t[kJBands];
+#pragma unroll
+      for (int i = 0; i < kJBands; ++i) t[i] = A(0);
+      for (int j0 = 0; j0 < bx; j0 += 32) {
+        const int j = j0 + lane;
+        A u[kJBands];
+#pragma unroll
+        for (int i = 0; i < kJBands; ++i) {
+          const int by = b0 + g * kJBands + i;
+          u[i] = tt[(size_t)min(by, p.nBY - 1) * p.nBX + min(j, p.nBX - 1)];
+        }
+#pragma unroll
+        for (int i = 0; i < kJBands; ++i)
+          if (j < bx && b0 + g * kJBands + i < p.nBY) t[i] += u[i];
+      }
+      const A tot = warp_sum_rows<kJBands>(t, lane);
+      if ((lane & (32 / kJBands - 1)) == 0)
+        band_left[g * kJBands + (lane >> (5 - log2_of<kJBands>()))] = tot;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kJBands; ++j) {
+      const int by = b0 + g * kJBands + j;
+      v[j] = (by < p.nBY && x < p.W) ? band_left[g * kJBands + j] + v[j] : A(0);
+    }
+    A s = A(0);
+#pragma unroll
+    for (int j = 0; j < kJBands; ++j) s += v[j];
+    group_total[g][lane] = s;
+    __syncthreads();
+    A run = carry;
+    for (int h = 0; h < g; ++h) run += group_total[h][lane];
+#pragma unroll
+    for (int j = 0; j < kJBands; ++j) {
+      const int by = b0 + g * kJBands + j;
+      if (by < p.nBY && x < p.W) lb[(size_t)by * p.W + x] = run;
+      run += v[j];
+    }
+#pragma unroll
+    for (int h = 0; h < kGroups; ++h) carry += group_total[h][lane];
+    __syncthreads();
   }
 }
 
@@ -177,9 +478,68 @@ __device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v);
 __device__ __forceinline__ double to_f64(long long v) { return __ll2double_rn(v); }
 __device__ __forceinline__ double to_f64(double v) { return v; }
 
-template <int TYPE, typename A, bool SQR>
-__global__ void __launch_bounds__(32 * kWarpsPerCta)
+// A 32-byte store of 4 doubles (sm_100 has 256-bit global accesses): a
+// warp's store covers 1 KB contiguous, every 32-byte sector written whole.
+__device__ __forceinline__ void st_global_v4f64(double* ptr, const double (&v)[4]) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(ptr), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+}
+
+// One row of the lane's 4 results: one vector store (32 bytes for F64, 16 for
+// F32) when the destination allows it.
+template <typename OT, typename A>
+__device__ __forceinline__ void store_row(const IntegralParams& p, int c, int y, int xl,
+                                          const A (&acc)[kPX]) {
+  OT* row = reinterpret_cast<OT*>(p.dst + (size_t)y * p.dst_pitch);
+  OT o[kPX];
+#pragma unroll
+  for (int k = 0; k < kPX; ++k) {
+    if constexpr (sizeof(OT) == 8) o[k] = to_f64(acc[k]);
+    else o[k] = to_f32(acc[k]);
+  }
+  if (p.vec_dst && xl + kPX <= p.W) {
+    if constexpr (sizeof(OT) == 8) {
+      st_global_v4f64(row + xl, o);
+    } else {
+      uint4 q;
+      memcpy(&q, o, sizeof(q));
+      *reinterpret_cast<uint4*>(row + xl) = q;
+    }
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < kPX; ++k)
+    if (xl + k < p.W) row[(size_t)(xl + k) * p.nch + c] = o[k];
+}
+
+// One row of the final pass: the lane's 4 values plus the row's RowLeft and
+// the warp-scanned prefix of the lanes to its left, added to the running
+// column sums and stored.
+template <typename A, bool SQR, typename OT, typename ET>
+__device__ __forceinline__ void final_row(const IntegralParams& p, int c, int y, int xl,
+                                          int lane, const ET (&e)[kPX], A left,
+                                          A (&acc)[kPX]) {
+  A v[kPX];
+#pragma unroll
+  for (int k = 0; k < kPX; ++k) v[k] = value_of<A, SQR>(e[k]);
+#pragma unroll
+  for (int k = 1; k < kPX; ++k) v[k] += v[k - 1];
+  const A incl = warp_incl_scan(v[kPX - 1], lane);
+  const A base = incl - v[kPX - 1] + left;
+#pragma unroll
+  for (int k = 0; k < kPX; ++k) acc[k] += base + v[k];
+  store_row<OT>(p, c, y, xl, acc);
+}
+
+static_assert(kTH <= 32, "a tile's RowLeft values are held one per lane");
+
+template <int TYPE, typename A, bool SQR, typename OT>
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
     integral_final_kernel(const IntegralParams p) {
+  using ET = typename ElemOf<TYPE>::T;
+  using RS = RowStream<ET>;
+  __shared__ __align__(16) unsigned char ring[kWarpsPerCta * RS::kWarpBytes];
   const int lane = threadIdx.x & 31;
   const int tile = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
   const int c = blockIdx.y;
@@ -187,47 +547,106 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta)
   const int bx = tile % p.nBX, by = tile / p.nBX;
   const int xl = bx * kTW + lane * kPX;
   const int y0 = by * kTH;
+  const int nrows = min(p.H, y0 + kTH) - y0;
   const A* rowleft = reinterpret_cast<const A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
   const A* top = reinterpret_cast<const A*>(p.lb) + (size_t)c * p.nBY * p.W;
+  const bool vec_tile = p.vec_src && (bx + 1) * kTW <= p.W;
+  const RS rs(ring + (threadIdx.x >> 5) * RS::kWarpBytes, lane,
+              p.src + (size_t)y0 * p.src_pitch + (size_t)xl * sizeof(ET), p.src_pitch, nrows);
+  // The first source rows are in flight while the junction launch (this
+  // kernel's programmatic predecessor) finishes; Top and RowLeft after it.
+  if (vec_tile) rs.start();
+  cudaGridDependencySynchronize();
   A acc[kPX];
 #pragma unroll
+  for (int k = 0; k < kPX; ++k) acc[k] = top[(size_t)by * p.W + min(xl + k, p.W - 1)];
+#pragma unroll
   for (int k = 0; k < kPX; ++k)
-    acc[k] = (xl + k < p.W) ? top[(size_t)by * p.W + xl + k] : A(0);
-  const int yend = min(p.H, y0 + kTH);
-  for (int y = y0; y < yend; ++y) {
-    A v[kPX];
-    load_row<TYPE, A, SQR>(p, c, y, xl, v);
+    if (xl + k >= p.W) acc[k] = A(0);
+  // RowLeft of the tile's rows: lane i holds row y0 + i.
+  const A left_lane = rowleft[(size_t)(y0 + min(lane, nrows - 1)) * p.nBX + bx];
+  if (vec_tile) {
+    for (int y = 0; y < nrows; ++y) {
+      ET e[kPX];
+      rs.read(y, e);
+      rs.refill(y);
+      final_row<A, SQR, OT>(p, c, y0 + y, xl, lane, e, __shfl_sync(0xffffffffu, left_lane, y),
+                            acc);
+    }
+    rs.drain();
+    return;
+  }
+  // Generic layouts (several channels, unaligned rows, the image's right
+  // edge): register groups of rows.
+  constexpr int G = group_rows<ET>() / 4;
+  for (int yg = 0; yg < nrows; yg += G) {
+    ET raw[G][kPX];
+    load_group<G>(p, c, y0 + yg, y0 + nrows, xl, false, raw);
 #pragma unroll
-    for (int k = 1; k < kPX; ++k) v[k] += v[k - 1];
-    const A incl = warp_incl_scan(v[kPX - 1], lane);
-    const A base = incl - v[kPX - 1] + rowleft[(size_t)y * p.nBX + bx];
-    char* drow = p.dst + (size_t)y * p.dst_pitch;
-#pragma unroll
-    for (int k = 0; k < kPX; ++k) {
-      acc[k] += base + v[k];
-      const int x = xl + k;
-      if (x < p.W) {
-        if (p.dst_f64)
-          reinterpret_cast<double*>(drow)[(size_t)x * p.nch + c] = to_f64(acc[k]);
-        else
-          reinterpret_cast<float*>(drow)[(size_t)x * p.nch + c] = to_f32(acc[k]);
-      }
+    for (int r = 0; r < G; ++r) {
+      const A left = __shfl_sync(0xffffffffu, left_lane, (yg + r) & 31);
+      if (yg + r < nrows) final_row<A, SQR, OT>(p, c, y0 + yg + r, xl, lane, raw[r], left, acc);
     }
   }
 }
 
+// Launch on st as a programmatic dependent of the previous launch on st: its
+// blocks may start as the previous launch's blocks exit, and
+// cudaGridDependencySynchronize() in the kernel waits for that launch's
+// completion and memory.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                             Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// Asks once per kernel for the largest shared-memory carveout: the row rings
+// take 16 KB per block and kMinCtas blocks should fit on an SM.
+template <typename K>
+void prefer_shared(K kernel) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    done = true;
+  }
+}
+
+// The reduce launch is an ordinary one: it overwrites the scratch that the
+// previous call's final launch reads.
 template <int TYPE, typename A, bool SQR>
 cudaError_t run(IntegralParams& p, cudaStream_t st) {
+  prefer_shared(integral_reduce_kernel<TYPE, A, SQR>);
+  prefer_shared(integral_final_kernel<TYPE, A, SQR, double>);
+  prefer_shared(integral_final_kernel<TYPE, A, SQR, float>);
   const int ntiles = p.nBX * p.nBY;
   dim3 g1((ntiles + kWarpsPerCta - 1) / kWarpsPerCta, p.nch);
   integral_reduce_kernel<TYPE, A, SQR><<<g1, 32 * kWarpsPerCta, 0, st>>>(p);
-  dim3 g2((p.H + p.nBY + 127) / 128, p.nch);
-  integral_junction_rows_kernel<A><<<g2, 128, 0, st>>>(p);
-  dim3 g3((p.W + 127) / 128, p.nch);
-  integral_junction_cols_kernel<A><<<g3, 128, 0, st>>>(p);
-  integral_final_kernel<TYPE, A, SQR><<<g1, 32 * kWarpsPerCta, 0, st>>>(p);
-  count_launches(4);
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int top_blocks = (p.W + kJCols - 1) / kJCols;
+  const int rows_per_block = kJThreads / 32 * kJRows;
+  dim3 g2(top_blocks + (p.H + rows_per_block - 1) / rows_per_block, p.nch);
+  e = launch_dependent(integral_junction_kernel<A>, g2, dim3(kJThreads), st, p, top_blocks);
+  if (e != cudaSuccess) return e;
+  if (p.dst_f64)
+    e = launch_dependent(integral_final_kernel<TYPE, A, SQR, double>, g1,
+                         dim3(32 * kWarpsPerCta), st, p);
+  else
+    e = launch_dependent(integral_final_kernel<TYPE, A, SQR, float>, g1,
+                         dim3(32 * kWarpsPerCta), st, p);
+  count_launches(3);
+  return e;
 }
 
 template <int TYPE, typename AI>
@@ -256,13 +675,17 @@ cudaError_t launch_integral(bool sqr, const DevImage& src, const DevImage& dst,
   p.nch = src.nch;
   p.nBX = (p.W + kTW - 1) / kTW;
   p.nBY = (p.H + kTH - 1) / kTH;
+  p.vec_src = p.nch == 1 && ((uintptr_t)p.src % 16) == 0 && (p.src_pitch % 16) == 0;
+  // A lane stores 4 pixels: 32 bytes for F64, 16 for F32.
+  const size_t dst_align = p.dst_f64 ? 32 : 16;
+  p.vec_dst = p.nch == 1 && ((uintptr_t)p.dst % dst_align) == 0 && (p.dst_pitch % dst_align) == 0;
   if (scratch_bytes < integral_scratch_bytes(p.W, p.H, p.nch)) return cudaErrorInvalidValue;
   char* s = (char*)scratch;
   p.rowsum = s;
   s += 8 * (size_t)p.nch * p.H * p.nBX;
   p.lb = s;
   s += 8 * (size_t)p.nch * p.nBY * p.W;
-  p.bandleft = s;
+  p.tt = s;
   switch (src.type) {
     case U8: return run_sqr<U8, long long>(sqr, p, st);
     case S8: return run_sqr<S8, long long>(sqr, p, st);
@@ -294,9 +717,9 @@ cudaError_t launch_integral(bool sqr, const DevImage& src, const DevImage& dst,
 namespace ocipb {
 namespace {
 
-// Largest scratch the allocation-free entry point can use: 8 MiB, enough for
-// one channel up to about 6000 x 6000 pixels (integral_scratch_bytes()).
-constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
+// Largest scratch the allocation-free entry point can use: 16 MiB, enough for
+// one channel up to about 7600 x 7600 pixels (integral_scratch_bytes()).
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
