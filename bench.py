@@ -782,7 +782,10 @@ def run_integral_bench(args, world, rank, local):
         "roofline": {"kernel": ["Integral", "SqrIntegral"][dom] + " (3 launches)",
                      "bound": "hbm", "achieved": round(gbs, 1), "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": round(gbs / peaks["hbm_gbs"], 4),
-                     "traffic": None, "peak_source": peaks["source"]},
+                     "traffic": ncu_traffic("Integral", "3 launches"),
+                     "traffic_note": "DRAM bytes of the three Integral launches, ncu with cold "
+                                     "caches (profiles/integral_f32_to_f64_4096x4096.md)",
+                     "peak_source": peaks["source"]},
         "e2e": {"value": round(bytes_step * world / (e2e_ms * 1e-3) / 1e9, 1), "unit": "GB/s",
                 "h2d_bytes_per_step": int(S.nbytes),
                 "d2h_bytes_per_step": int(sum(o.nbytes for o in houts))},

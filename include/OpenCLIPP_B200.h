@@ -63,7 +63,7 @@ ocipError ocip_API ocipGetLaunchCount(uint64_t* Count);
  * calling thread's current CUDA device, and no context is needed.
  * The scan's scratch is a fixed 16 MiB array that every device which loads
  * the library holds until the process exits; images whose scratch would not
- * fit (about 7600 x 7600 pixels per channel) are refused with
+ * fit (about 7300 x 7300 pixels per channel) are refused with
  * CL_INVALID_IMAGE_SIZE. The first call on a device looks up that array's
  * device address; make that first call before capturing the stream into a
  * CUDA graph. All calls share the array: calls that overlap on the GPU (on

@@ -16,16 +16,18 @@
 // (4 for 8-byte types) before it sums any of them, and the kernels stay
 // within 64 registers so that 32 warps share an SM: a 4096 x 4096 image is
 // 4096 tiles, all resident at once on 148 SMs. Three launches:
-//   1. tile reduce (reads the source): per-row tile sums (RowSum), the tile's
-//      local integral at its bottom row (LB) and the tile's total (TT) -- the
-//      counterpart of the reference's vertical/horizontal junction buffers;
-//   2. junctions, one launch with two kinds of blocks: a warp per row turns
-//      RowSum into RowLeft (exclusive scan across the tiles of the row), and
-//      blocks of 32 columns turn LB into Top (exclusive scan over bands of
-//      BandLeft + LB, BandLeft = the band's tile totals left of the column's
-//      tile), which is the full integral of the row just above each band;
+//   1. tile reduce (reads the source): per-row tile sums (RowSum) and the
+//      tile's local integral at its bottom row (LB) -- the counterpart of the
+//      reference's vertical/horizontal junction buffers;
+//   2. junctions, one launch with two kinds of blocks: blocks of 32 columns
+//      turn LB into ColTop (exclusive scan of LB over the bands), and warps
+//      turn RowSum into RowLeft (exclusive scan across the tiles of a row);
 //   3. final (reads the source again, mostly from L2): D = Top + running sum
-//      over the band's rows of (RowLeft + warp-scanned row prefix).
+//      over the band's rows of (RowLeft + warp-scanned row prefix), where the
+//      integral of the row above the band is Top(x) = ColTop(x) + the sum of
+//      ColTop at the last column of every tile left of x (LB at a tile's last
+//      column is the tile's total, so that sum is the integral of the tiles
+//      left of this one over the bands above).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -41,8 +43,8 @@ constexpr int kPX = 4;     // columns per lane
 constexpr int kWarpsPerCta = 4;
 constexpr int kMinCtas = 8;      // 32 warps per SM: at most 64 registers
 constexpr int kJThreads = 256;   // junction blocks
-constexpr int kJCols = 32;       // columns per Top block
-constexpr int kJBands = 16;      // bands per thread and chunk step in a Top block
+constexpr int kJCols = 32;       // columns per ColTop block
+constexpr int kJBands = 16;      // bands per thread and chunk step in a ColTop block
 constexpr int kJRows = 8;        // image rows per warp in a RowLeft block
 
 template <int TYPE> struct ElemOf;
@@ -66,8 +68,7 @@ struct IntegralParams {
   int vec_src;     // 1: one channel, 16-byte aligned base and pitch
   int vec_dst;     // 1: one channel, base and pitch aligned to a lane's 4 pixels
   void* rowsum;    // [nch][H][nBX]     RowSum, then RowLeft
-  void* lb;        // [nch][nBY][W]     LB, then Top
-  void* tt;        // [nch][nBY][nBX]   tile totals
+  void* lb;        // [nch][nBY][W]     LB, then ColTop
 };
 
 template <typename A>
@@ -294,7 +295,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
   const int y0 = by * kTH;
   A* rowsum = reinterpret_cast<A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
   A* lb = reinterpret_cast<A*>(p.lb) + (size_t)c * p.nBY * p.W;
-  A* tt = reinterpret_cast<A*>(p.tt) + (size_t)c * p.nBY * p.nBX;
   A col[kPX];
 #pragma unroll
   for (int k = 0; k < kPX; ++k) col[k] = A(0);
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
     }
   }
   // Tile-local prefix of the column sums along x = the tile's local integral
-  // at its bottom row; lane 31's inclusive value is the tile's total.
+  // at its bottom row.
 #pragma unroll
   for (int k = 1; k < kPX; ++k) col[k] += col[k - 1];
   const A incl = warp_incl_scan(col[kPX - 1], lane);
@@ -363,21 +363,21 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
 #pragma unroll
   for (int k = 0; k < kPX; ++k)
     if (xl + k < p.W) lb[(size_t)by * p.W + xl + k] = excl + col[k];
-  if (lane == 31) tt[(size_t)by * p.nBX + bx] = incl;
 }
 
-// Junctions. Blocks [0, top_blocks): kJCols columns each (inside one tile
-// column, since kJCols divides kTW), LB -> Top in place, bands taken in chunks
-// of 8 x kJBands: thread (column, group g) loads kJBands bands, the groups'
-// totals are combined through shared memory. These blocks have the longer
-// dependency chain, so they come first in the grid. Blocks after them: a
-// warp per kJRows image rows, RowSum -> RowLeft in place.
+// Junctions. Blocks [0, top_blocks): kJCols columns each, LB -> ColTop in
+// place, bands taken in chunks of 8 x kJBands: thread (column, group g) loads
+// kJBands bands, the groups' totals are combined through shared memory. These
+// blocks have the longer dependency chain, so they come first in the grid.
+// Blocks after them: a warp per kJRows image rows, RowSum -> RowLeft in place.
+// Loads are issued from clamped (always valid) addresses and masked
+// afterwards: a load whose use sits in the same branch would stall the warp
+// before the next load issues.
 template <typename A>
-__global__ void __launch_bounds__(kJThreads, 2)
+__global__ void __launch_bounds__(kJThreads)
     integral_junction_kernel(const IntegralParams p, int top_blocks) {
   constexpr int kGroups = kJThreads / kJCols;
   constexpr int kChunk = kGroups * kJBands;
-  __shared__ A band_left[kChunk];
   __shared__ A group_total[kGroups][kJCols];
   const int c = blockIdx.y;
   const int lane = threadIdx.x & 31;
@@ -385,7 +385,6 @@ __global__ void __launch_bounds__(kJThreads, 2)
   // read here is written by it.
   cudaGridDependencySynchronize();
   if ((int)blockIdx.x >= top_blocks) {
-    // kJRows rows per warp, their loads issued together (clamped addresses).
     const int y0 = ((blockIdx.x - top_blocks) * (kJThreads / 32) + (threadIdx.x >> 5)) * kJRows;
     if (y0 >= p.H) return;
     A* rs = reinterpret_cast<A*>(p.rowsum) + (size_t)c * p.H * p.nBX;
@@ -409,54 +408,21 @@ __global__ void __launch_bounds__(kJThreads, 2)
     return;
   }
   A* lb = reinterpret_cast<A*>(p.lb) + (size_t)c * p.nBY * p.W;
-  const A* tt = reinterpret_cast<const A*>(p.tt) + (size_t)c * p.nBY * p.nBX;
-  const int x0 = blockIdx.x * kJCols;
-  const int x = x0 + lane;
+  const int x = blockIdx.x * kJCols + lane;
+  const int xc = min(x, p.W - 1);
   const int g = threadIdx.x >> 5;
-  const int bx = x0 / kTW;
   A carry = A(0);
   for (int b0 = 0; b0 < p.nBY; b0 += kChunk) {
-    // This thread's LB values (column x, bands g * kJBands + j), issued first
-    // so that they are in flight while BandLeft is summed. Clamped (always
-    // valid) addresses, masked afterwards: a load whose use sits in the same
-    // branch would stall the warp before the next load issues.
     A v[kJBands];
-    const int xc = min(x, p.W - 1);
 #pragma unroll
     for (int j = 0; j < kJBands; ++j)
       v[j] = lb[(size_t)min(b0 + g * kJBands + j, p.nBY - 1) * p.W + xc];
-    {
-      // BandLeft of the warp's bands g * kJBands .. + kJBands - 1: the tile
-      // totals left of this tile, lane j taking tile columns j, j + 32, ...;
-      // one multi-row warp reduction combines them. Only warp g reads them.
-      A t[kJBands];
-#pragma unroll
-      for (int i = 0; i < kJBands; ++i) t[i] = A(0);
-      for (int j0 = 0; j0 < bx; j0 += 32) {
-        const int j = j0 + lane;
-        A u[kJBands];
-#pragma unroll
-        for (int i = 0; i < kJBands; ++i) {
-          const int by = b0 + g * kJBands + i;
-          u[i] = tt[(size_t)min(by, p.nBY - 1) * p.nBX + min(j, p.nBX - 1)];
-        }
-#pragma unroll
-        for (int i = 0; i < kJBands; ++i)
-          if (j < bx && b0 + g * kJBands + i < p.nBY) t[i] += u[i];
-      }
-      const A tot = warp_sum_rows<kJBands>(t, lane);
-      if ((lane & (32 / kJBands - 1)) == 0)
-        band_left[g * kJBands + (lane >> (5 - log2_of<kJBands>()))] = tot;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < kJBands; ++j) {
-      const int by = b0 + g * kJBands + j;
-      v[j] = (by < p.nBY && x < p.W) ? band_left[g * kJBands + j] + v[j] : A(0);
-    }
     A s = A(0);
 #pragma unroll
-    for (int j = 0; j < kJBands; ++j) s += v[j];
+    for (int j = 0; j < kJBands; ++j) {
+      if (b0 + g * kJBands + j >= p.nBY) v[j] = A(0);
+      s += v[j];
+    }
     group_total[g][lane] = s;
     __syncthreads();
     A run = carry;
@@ -557,12 +523,21 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kMinCtas)
   // kernel's programmatic predecessor) finishes; Top and RowLeft after it.
   if (vec_tile) rs.start();
   cudaGridDependencySynchronize();
+  // Top = ColTop + the sum of ColTop at the last column of the tiles to the
+  // left (lane j takes tiles j, j + 32, ...).
+  A left_tiles = A(0);
+  for (int j0 = 0; j0 < bx; j0 += 32) {
+    const int j = min(j0 + lane, bx - 1);
+    const A v = top[(size_t)by * p.W + min(p.W, (j + 1) * kTW) - 1];
+    if (j0 + lane < bx) left_tiles += v;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) left_tiles += __shfl_xor_sync(0xffffffffu, left_tiles, d);
   A acc[kPX];
 #pragma unroll
   for (int k = 0; k < kPX; ++k) acc[k] = top[(size_t)by * p.W + min(xl + k, p.W - 1)];
 #pragma unroll
-  for (int k = 0; k < kPX; ++k)
-    if (xl + k >= p.W) acc[k] = A(0);
+  for (int k = 0; k < kPX; ++k) acc[k] = (xl + k < p.W) ? acc[k] + left_tiles : A(0);
   // RowLeft of the tile's rows: lane i holds row y0 + i.
   const A left_lane = rowleft[(size_t)(y0 + min(lane, nrows - 1)) * p.nBX + bx];
   if (vec_tile) {
@@ -658,7 +633,7 @@ cudaError_t run_sqr(bool sqr, IntegralParams& p, cudaStream_t st) {
 
 size_t integral_scratch_bytes(int width, int height, int nch) {
   const size_t nBX = (width + kTW - 1) / kTW, nBY = (height + kTH - 1) / kTH;
-  return 8 * (size_t)nch * ((size_t)height * nBX + nBY * (size_t)width + nBY * nBX) + 256;
+  return 8 * (size_t)nch * ((size_t)height * nBX + nBY * (size_t)width) + 256;
 }
 
 cudaError_t launch_integral(bool sqr, const DevImage& src, const DevImage& dst,
@@ -684,8 +659,7 @@ cudaError_t launch_integral(bool sqr, const DevImage& src, const DevImage& dst,
   p.rowsum = s;
   s += 8 * (size_t)p.nch * p.H * p.nBX;
   p.lb = s;
-  s += 8 * (size_t)p.nch * p.nBY * p.W;
-  p.tt = s;
+
   switch (src.type) {
     case U8: return run_sqr<U8, long long>(sqr, p, st);
     case S8: return run_sqr<S8, long long>(sqr, p, st);
@@ -718,7 +692,7 @@ namespace ocipb {
 namespace {
 
 // Largest scratch the allocation-free entry point can use: 16 MiB, enough for
-// one channel up to about 7600 x 7600 pixels (integral_scratch_bytes()).
+// one channel up to about 7300 x 7300 pixels (integral_scratch_bytes()).
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
