@@ -62,6 +62,58 @@ __device__ __forceinline__ uint32_t shifted(uint32_t lo, uint32_t hi, int k) {
   return __byte_perm(lo, hi, 0x3210 + 0x1111 * k);
 }
 
+// One staged source row q (r = q - first row of the warp) applied to the
+// warp's RY output rows. FULL: every output row j meets template row
+// h = r - j (no range checks).
+template <bool FULL>
+__device__ __forceinline__ void sad_row(const SadParams& p, const unsigned char* s_src,
+                                        const unsigned char* s_t, int q, int r, int nc,
+                                        int lane, uint32_t mlast0, uint32_t mlast1,
+                                        uint32_t (&acc)[RY][RX]) {
+  const unsigned char* srow = s_src + (size_t)q * p.rowB + lane * RX;
+  for (int ch = 0; ch < nc; ++ch) {
+    const uint2 a = *reinterpret_cast<const uint2*>(srow + 8 * ch);
+    const uint2 b = *reinterpret_cast<const uint2*>(srow + 8 * ch + 8);
+    uint32_t sw[12];
+    sw[0] = a.x;
+    sw[4] = a.y;
+    sw[8] = b.x;
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+      sw[k] = shifted(a.x, a.y, k);
+      sw[4 + k] = shifted(a.y, b.x, k);
+      sw[8 + k] = shifted(b.x, b.y, k);
+    }
+    // Output i reads word i against template bytes 0 .. 3 of the chunk and
+    // word i + 4 against bytes 4 .. 7; in the last chunk each is masked to
+    // the valid bytes it meets.
+    uint32_t w0[RX], w1[RX];
+#pragma unroll
+    for (int i = 0; i < RX; ++i) {
+      w0[i] = sw[i];
+      w1[i] = sw[i + 4];
+    }
+    if (ch == nc - 1) {
+#pragma unroll
+      for (int i = 0; i < RX; ++i) {
+        w0[i] &= mlast0;
+        w1[i] &= mlast1;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < RY; ++j) {
+      const int h = r - j;
+      if (!FULL && (h < 0 || h >= p.th)) continue;
+      const uint2 t = *reinterpret_cast<const uint2*>(s_t + (size_t)h * p.tw8 + 8 * ch);
+#pragma unroll
+      for (int i = 0; i < RX; ++i) {
+        acc[j][i] = sad4(w0[i], t.x, acc[j][i]);
+        acc[j][i] = sad4(w1[i], t.y, acc[j][i]);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) prox_sad_u8_kernel(const SadParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
@@ -119,59 +171,19 @@ __global__ void __launch_bounds__(kThreads) prox_sad_u8_kernel(const SadParams p
   const uint32_t mlast0 = rem >= 4 ? 0xffffffffu : (1u << (8 * rem)) - 1u;
   const uint32_t mlast1 = rem >= 8 ? 0xffffffffu : rem <= 4 ? 0u : (1u << (8 * (rem - 4))) - 1u;
 
+  // Staged rows q of this warp: r = q - warp * RY in [0, RY + th - 1). Rows
+  // with r in [RY - 1, th - 1] meet a template row in every output row of
+  // the warp and take the loop without range checks.
   const int qa = warp * RY;
   const int qb = min(qtot, warp * RY + RY + p.th - 1);
-  for (int q = qa; q < qb; ++q) {
-    const int r = q - warp * RY;
-    const unsigned char* srow = s_src + (size_t)q * p.rowB + lane * RX;
-    for (int ch = 0; ch < nc; ++ch) {
-      const uint2 a = *reinterpret_cast<const uint2*>(srow + 8 * ch);
-      const uint2 b = *reinterpret_cast<const uint2*>(srow + 8 * ch + 8);
-      uint32_t sw[12];
-      sw[0] = a.x;
-      sw[4] = a.y;
-      sw[8] = b.x;
-#pragma unroll
-      for (int k = 1; k < 4; ++k) {
-        sw[k] = shifted(a.x, a.y, k);
-        sw[4 + k] = shifted(a.y, b.x, k);
-        sw[8 + k] = shifted(b.x, b.y, k);
-      }
-      if (ch == nc - 1) {
-        // Output i reads words i (template bytes 0 .. 3 of the chunk) and
-        // i + 4 (bytes 4 .. 7); mask each by the valid bytes it meets.
-        uint32_t w0[RX], w1[RX];
-#pragma unroll
-        for (int i = 0; i < RX; ++i) {
-          w0[i] = sw[i] & mlast0;
-          w1[i] = sw[i + 4] & mlast1;
-        }
-#pragma unroll
-        for (int j = 0; j < RY; ++j) {
-          const int h = r - j;
-          if (h < 0 || h >= p.th) continue;
-          const uint2 t = *reinterpret_cast<const uint2*>(s_t + (size_t)h * p.tw8 + 8 * ch);
-#pragma unroll
-          for (int i = 0; i < RX; ++i) {
-            acc[j][i] = sad4(w0[i], t.x, acc[j][i]);
-            acc[j][i] = sad4(w1[i], t.y, acc[j][i]);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < RY; ++j) {
-          const int h = r - j;
-          if (h < 0 || h >= p.th) continue;
-          const uint2 t = *reinterpret_cast<const uint2*>(s_t + (size_t)h * p.tw8 + 8 * ch);
-#pragma unroll
-          for (int i = 0; i < RX; ++i) {
-            acc[j][i] = sad4(sw[i], t.x, acc[j][i]);
-            acc[j][i] = sad4(sw[i + 4], t.y, acc[j][i]);
-          }
-        }
-      }
-    }
-  }
+  const int fa = min(qb, qa + RY - 1);
+  const int fb = max(fa, min(qb, qa + p.th));
+  for (int q = qa; q < fa; ++q)
+    sad_row<false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
+  for (int q = fa; q < fb; ++q)
+    sad_row<true>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
+  for (int q = fb; q < qb; ++q)
+    sad_row<false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
 
 #pragma unroll
   for (int j = 0; j < RY; ++j) {
