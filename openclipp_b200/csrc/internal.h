@@ -50,12 +50,12 @@ cudaError_t launch_proximity_plain(Measure m, const DevImage& src,
                                    const DevImage& tmpl, const DevImage& dst,
                                    void* tt_scratch, cudaStream_t stream);
 
-// AbsDistance of a U8 source with packed-byte SAD (four taps per instruction,
-// exact uint32 sums); launch_proximity_plain routes U8 AbsDistance here when
-// proximity_sad_u8_supported() holds.
-size_t proximity_sad_u8_smem(int tw, int th);
-bool proximity_sad_u8_supported(const DevImage& src, const DevImage& tmpl);
-cudaError_t launch_proximity_sad_u8(const DevImage& src, const DevImage& tmpl,
+// AbsDistance of a U8 or S8 source with packed-byte SAD (four taps per
+// instruction, exact uint32 sums); launch_proximity_plain routes 8-bit
+// AbsDistance here when proximity_sad_8bit_supported() holds.
+size_t proximity_sad_8bit_smem(int tw, int th);
+bool proximity_sad_8bit_supported(const DevImage& src, const DevImage& tmpl);
+cudaError_t launch_proximity_sad_8bit(const DevImage& src, const DevImage& tmpl,
                                     const DevImage& dst, cudaStream_t stream);
 
 // Scratch for the integral scan: per-row tile sums and per-band column

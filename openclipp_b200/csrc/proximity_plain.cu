@@ -375,8 +375,8 @@ cudaError_t launch_proximity_plain(Measure m, const DevImage& src,
                                    const DevImage& tmpl, const DevImage& dst,
                                    void* tt_scratch, cudaStream_t st) {
   const int area = tmpl.width * tmpl.height;
-  if (m == kAbsDistance && proximity_sad_u8_supported(src, tmpl))
-    return launch_proximity_sad_u8(src, tmpl, dst, st);
+  if (m == kAbsDistance && proximity_sad_8bit_supported(src, tmpl))
+    return launch_proximity_sad_8bit(src, tmpl, dst, st);
   switch (src.type) {
     case U8:
       return small_int_exact_in_float(m, area)

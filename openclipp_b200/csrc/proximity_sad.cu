@@ -1,14 +1,15 @@
-// Packed-byte SAD kernel for AbsDistance of 8-bit unsigned sources, sm_100a.
+// Packed-byte SAD kernel for AbsDistance of 8-bit sources (U8, S8), sm_100a.
 //
 // AbsDistance (reference cl-files/ImageProximity.cl:213-242) sums |S - T| over
-// the window. For a U8 source every term is an integer in [0, 255], so the sum
+// the window. For an 8-bit source every term is an integer in [0, 255], so the sum
 // is exact in a uint32 register for any template of fewer than 2^24 pixels,
 // and the result is rounded once to the destination type. That equals the
 // plain kernel's result (float accumulation while sums stay below 2^24, exact
 // double above) and the reference's wherever its float accumulation is exact.
 //
 // Four taps per instruction: vabsdiff4 with accumulate adds the four bytewise
-// absolute differences of two packed words to a 32-bit sum.
+// absolute differences of two packed words (bytes unsigned for U8, signed for
+// S8) to a 32-bit sum.
 //
 // Tiling follows the plain kernel: a CTA of 8 warps owns a 256 x 32 output
 // tile; lane l owns 8 consecutive columns, warp w owns 4 consecutive rows.
@@ -50,10 +51,15 @@ struct SadParams {
   int rowB;   // bytes per staged source row (multiple of 16)
 };
 
-// acc + |a0 - b0| + |a1 - b1| + |a2 - b2| + |a3 - b3| over the bytes of a, b.
+// acc + |a0 - b0| + |a1 - b1| + |a2 - b2| + |a3 - b3| over the bytes of a, b
+// (unsigned bytes, or signed bytes when SIGNED).
+template <bool SIGNED>
 __device__ __forceinline__ uint32_t sad4(uint32_t a, uint32_t b, uint32_t acc) {
   uint32_t d;
-  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(acc));
+  if constexpr (SIGNED)
+    asm("vabsdiff4.u32.s32.s32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(acc));
+  else
+    asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(acc));
   return d;
 }
 
@@ -65,7 +71,7 @@ __device__ __forceinline__ uint32_t shifted(uint32_t lo, uint32_t hi, int k) {
 // One staged source row q (r = q - first row of the warp) applied to the
 // warp's RY output rows. FULL: every output row j meets template row
 // h = r - j (no range checks).
-template <bool FULL>
+template <bool SIGNED, bool FULL>
 __device__ __forceinline__ void sad_row(const SadParams& p, const unsigned char* s_src,
                                         const unsigned char* s_t, int q, int r, int nc,
                                         int lane, uint32_t mlast0, uint32_t mlast1,
@@ -107,14 +113,15 @@ __device__ __forceinline__ void sad_row(const SadParams& p, const unsigned char*
       const uint2 t = *reinterpret_cast<const uint2*>(s_t + (size_t)h * p.tw8 + 8 * ch);
 #pragma unroll
       for (int i = 0; i < RX; ++i) {
-        acc[j][i] = sad4(w0[i], t.x, acc[j][i]);
-        acc[j][i] = sad4(w1[i], t.y, acc[j][i]);
+        acc[j][i] = sad4<SIGNED>(w0[i], t.x, acc[j][i]);
+        acc[j][i] = sad4<SIGNED>(w1[i], t.y, acc[j][i]);
       }
     }
   }
 }
 
-__global__ void __launch_bounds__(kThreads) prox_sad_u8_kernel(const SadParams p) {
+template <bool SIGNED>
+__global__ void __launch_bounds__(kThreads) prox_sad_kernel(const SadParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -179,11 +186,11 @@ __global__ void __launch_bounds__(kThreads) prox_sad_u8_kernel(const SadParams p
   const int fa = min(qb, qa + RY - 1);
   const int fb = max(fa, min(qb, qa + p.th));
   for (int q = qa; q < fa; ++q)
-    sad_row<false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
+    sad_row<SIGNED, false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
   for (int q = fa; q < fb; ++q)
-    sad_row<true>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
+    sad_row<SIGNED, true>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
   for (int q = fb; q < qb; ++q)
-    sad_row<false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
+    sad_row<SIGNED, false>(p, s_src, s_t, q, q - qa, nc, lane, mlast0, mlast1, acc);
 
 #pragma unroll
   for (int j = 0; j < RY; ++j) {
@@ -204,20 +211,20 @@ __global__ void __launch_bounds__(kThreads) prox_sad_u8_kernel(const SadParams p
 
 }  // namespace
 
-size_t proximity_sad_u8_smem(int tw, int th) {
+size_t proximity_sad_8bit_smem(int tw, int th) {
   const int tw8 = (tw + 7) / 8 * 8;
   const int rowB = (TX + tw8 + 15) / 16 * 16;
   return (size_t)(TY + th - 1) * rowB + (size_t)th * tw8;
 }
 
-bool proximity_sad_u8_supported(const DevImage& src, const DevImage& tmpl) {
-  if (src.type != U8 || tmpl.type != U8) return false;
+bool proximity_sad_8bit_supported(const DevImage& src, const DevImage& tmpl) {
+  if ((src.type != U8 && src.type != S8) || tmpl.type != src.type) return false;
   // Exact uint32 sums: every output adds tw * th terms of at most 255.
   if ((double)tmpl.width * tmpl.height * 255.0 >= 4294967296.0) return false;
-  return proximity_sad_u8_smem(tmpl.width, tmpl.height) <= (size_t)kSmemBudget;
+  return proximity_sad_8bit_smem(tmpl.width, tmpl.height) <= (size_t)kSmemBudget;
 }
 
-cudaError_t launch_proximity_sad_u8(const DevImage& src, const DevImage& tmpl,
+cudaError_t launch_proximity_sad_8bit(const DevImage& src, const DevImage& tmpl,
                                     const DevImage& dst, cudaStream_t st) {
   SadParams p;
   p.src = (const unsigned char*)src.ptr;
@@ -235,12 +242,13 @@ cudaError_t launch_proximity_sad_u8(const DevImage& src, const DevImage& tmpl,
   p.th = tmpl.height;
   p.tw8 = (p.tw + 7) / 8 * 8;
   p.rowB = (TX + p.tw8 + 15) / 16 * 16;
-  const size_t smem = proximity_sad_u8_smem(p.tw, p.th);
-  cudaError_t e = cudaFuncSetAttribute(prox_sad_u8_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = proximity_sad_8bit_smem(p.tw, p.th);
+  auto kern = src.type == S8 ? prox_sad_kernel<true> : prox_sad_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((p.W + TX - 1) / TX, (p.H + TY - 1) / TY, src.nch);
-  prox_sad_u8_kernel<<<grid, kThreads, smem, st>>>(p);
+  kern<<<grid, kThreads, smem, st>>>(p);
   count_launches(1);
   return cudaGetLastError();
 }

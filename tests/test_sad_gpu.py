@@ -1,4 +1,5 @@
-"""AbsDistance of U8 sources: the packed-byte SAD kernel against the oracle.
+"""AbsDistance of 8-bit sources (U8, S8): the packed-byte SAD kernel against
+the oracle.
 
 Every |S - T| of an 8-bit source is an integer in [0, 255], so the kernel's
 uint32 sums are exact; the result must equal the exact sum rounded once to
@@ -19,30 +20,38 @@ def exact_abs(S, T, out_dtype):
     return O.proximity_exact(2, S, T).astype(out_dtype)
 
 
+def rand8(rng, shape, dtype):
+    info = np.iinfo(dtype)
+    return rng.integers(info.min, int(info.max) + 1, shape).astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.int8])
 @pytest.mark.parametrize("tw", [1, 3, 4, 5, 7, 8, 9, 15, 17, 31, 33])
-def test_template_widths(ocip, plain, tw):
+def test_template_widths(ocip, plain, tw, dtype):
     rng = np.random.default_rng(700 + tw)
-    S = rng.integers(0, 256, (77, 301), dtype=np.uint8)
-    T = rng.integers(0, 256, (6, tw), dtype=np.uint8)
+    S = rand8(rng, (77, 301), dtype)
+    T = rand8(rng, (6, tw), dtype)
     got = ocip.match("AbsDistance", S, T)
     assert np.array_equal(got, exact_abs(S, T, np.float32))
 
 
+@pytest.mark.parametrize("dtype", [np.uint8, np.int8])
 @pytest.mark.parametrize("W,H,tw,th", [(1, 1, 1, 1), (256, 32, 16, 16), (257, 33, 16, 16),
                                        (600, 70, 31, 31), (40, 300, 7, 40)])
-def test_image_edges(ocip, plain, W, H, tw, th):
+def test_image_edges(ocip, plain, W, H, tw, th, dtype):
     rng = np.random.default_rng(W * 1000 + H)
-    S = rng.integers(0, 256, (H, W), dtype=np.uint8)
-    T = rng.integers(0, 256, (th, tw), dtype=np.uint8)
+    S = rand8(rng, (H, W), dtype)
+    T = rand8(rng, (th, tw), dtype)
     got = ocip.match("AbsDistance", S, T)
     assert np.array_equal(got, exact_abs(S, T, np.float32))
 
 
+@pytest.mark.parametrize("dtype", [np.uint8, np.int8])
 @pytest.mark.parametrize("nch", [2, 4])
-def test_channels_and_f64_destination(ocip, plain, nch):
+def test_channels_and_f64_destination(ocip, plain, nch, dtype):
     rng = np.random.default_rng(40 + nch)
-    S = rng.integers(0, 256, (45, 270, nch), dtype=np.uint8)
-    T = rng.integers(0, 256, (11, 13, nch), dtype=np.uint8)
+    S = rand8(rng, (45, 270, nch), dtype)
+    T = rand8(rng, (11, 13, nch), dtype)
     assert np.array_equal(ocip.match("AbsDistance", S, T), exact_abs(S, T, np.float32))
     assert np.array_equal(ocip.match("AbsDistance", S, T, np.float64),
                           exact_abs(S, T, np.float64))
@@ -68,6 +77,16 @@ def test_all_terms_255_and_sums_beyond_float(ocip, plain, H, W, th, tw):
     assert want.max() > 2**24
     got = ocip.match("AbsDistance", S, T)
     assert np.array_equal(got, want.astype(np.float32))
+
+
+def test_s8_extremes(ocip, plain):
+    """-128 against 127 gives the largest signed term, 255, in every tap."""
+    S = np.full((40, 300), -128, np.int8)
+    S[:, 1::2] = 127
+    T = np.full((9, 21), 127, np.int8)
+    T[::2] = -128
+    got = ocip.match("AbsDistance", S, T)
+    assert np.array_equal(got, exact_abs(S, T, np.float32))
 
 
 def test_matches_reference_kernel(ocip, plain):
