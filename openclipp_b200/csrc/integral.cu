@@ -12,10 +12,11 @@
 //
 // Layout: the image is cut into 128 x 32 tiles, one warp per tile (lane l
 // holds 4 consecutive columns, so one vector load of a warp reads 128
-// contiguous pixels when the image allows it). A warp loads a group of 8 rows
-// (4 for 8-byte types) before it sums any of them, and the kernels stay
-// within 64 registers so that 32 warps share an SM: a 4096 x 4096 image is
-// 4096 tiles, all resident at once on 148 SMs. Three launches:
+// contiguous pixels when the image allows it). On that vector path the tile's
+// rows stream through a per-lane cp.async ring in shared memory (RowStream);
+// other layouts load groups of rows into registers. The kernels stay within
+// 64 registers so that 32 warps share an SM: a 4096 x 4096 image is 4096
+// tiles, all resident at once on 148 SMs. Three launches:
 //   1. tile reduce (reads the source): per-row tile sums (RowSum) and the
 //      tile's local integral at its bottom row (LB) -- the counterpart of the
 //      reference's vertical/horizontal junction buffers;
@@ -111,7 +112,9 @@ __device__ __forceinline__ A warp_sum_rows(A (&s)[G], int lane) {
 template <int G>
 __host__ __device__ constexpr int log2_of() { return G <= 1 ? 0 : 1 + log2_of<G / 2>(); }
 
-// Rows a warp loads before it consumes any: 4 KB per warp for 4-byte types.
+// Rows whose tile sums one multi-row warp reduction combines in the reduce
+// pass (8, or 4 for 8-byte types); the register paths load a group of rows
+// before they use any of them.
 template <typename ET>
 __host__ __device__ constexpr int group_rows() { return sizeof(ET) >= 8 ? 4 : 8; }
 
