@@ -32,6 +32,9 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "internal.h"
 
@@ -588,25 +591,27 @@ cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, cu
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// Asks once per kernel for the largest shared-memory carveout: the row rings
-// take 16 KB per block and kMinCtas blocks should fit on an SM.
-template <typename K>
-void prefer_shared(K kernel) {
-  static bool done = false;
-  if (!done) {
+// Asks for the largest shared-memory carveout for `kernel` on the current
+// device, once per (kernel, device): the row rings take 16 KB per block and
+// kMinCtas blocks should fit on an SM.
+void prefer_shared(const void* kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.insert({kernel, dev}).second)
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    done = true;
-  }
 }
 
 // The reduce launch is an ordinary one: it overwrites the scratch that the
 // previous call's final launch reads.
 template <int TYPE, typename A, bool SQR>
 cudaError_t run(IntegralParams& p, cudaStream_t st) {
-  prefer_shared(integral_reduce_kernel<TYPE, A, SQR>);
-  prefer_shared(integral_final_kernel<TYPE, A, SQR, double>);
-  prefer_shared(integral_final_kernel<TYPE, A, SQR, float>);
+  prefer_shared((const void*)integral_reduce_kernel<TYPE, A, SQR>);
+  prefer_shared((const void*)integral_final_kernel<TYPE, A, SQR, double>);
+  prefer_shared((const void*)integral_final_kernel<TYPE, A, SQR, float>);
   const int ntiles = p.nBX * p.nBY;
   dim3 g1((ntiles + kWarpsPerCta - 1) / kWarpsPerCta, p.nch);
   integral_reduce_kernel<TYPE, A, SQR><<<g1, 32 * kWarpsPerCta, 0, st>>>(p);
