@@ -23,6 +23,11 @@ throughput is the sum of the ranks' taps over the slowest rank's time
 --impl reference times the reference's own kernel source
 (cl-files/ImageProximity.cl, compiled for the host, oracle/_ref) on the host
 cores on a band of rows of the same workload.
+
+Other workloads (--workload): batch (16 x 2048^2 U8 images x 64 uneven
+templates in persistent launches), backward (gradients vs forward time on 32 x
+1024^2 F32), integral (4096^2 F32 -> F64 Integral + SqrIntegral, GB/s against
+the HBM peak) and sad (4096^2 U8 AbsDistance on packed-byte SAD).
 """
 import argparse
 import json
