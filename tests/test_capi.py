@@ -115,3 +115,19 @@ int main(void) {
         assert first in ("SUCCESS", "CL_DEVICE_NOT_FOUND")
         if first == "SUCCESS":
             assert r.stdout.split()[1] == "SUCCESS"
+
+
+def test_no_alloc_scratch_limit_is_checked_on_the_host(ocip):
+    """ocipIntegralNoAlloc refuses an image whose scan scratch exceeds its fixed
+    16 MiB array before any device work: one channel fits up to 7307 x 7307
+    (8 bytes per 128-pixel row segment and per column of each 32-row band),
+    7308 x 7308 does not. Only refused sizes are passed here, so the dummy
+    pointers are never used."""
+    import ctypes
+    for w, h in ((7308, 7308), (100000, 1000), (1000, 100000)):
+        src = ocip.SImage(w, h, w, 1, ocip.U8)
+        dst = ocip.SImage(w, h, w * 8, 1, ocip.F64)
+        rc = ocip.lib.ocipIntegralNoAlloc(1, src, ctypes.c_void_p(16), w, dst,
+                                          ctypes.c_void_p(16), w * 8, None)
+        assert rc == ocip.CL_INVALID_IMAGE_SIZE, (w, h, rc)
+        assert b"fixed limit" in ocip.lib.ocipGetLastErrorMessage()
