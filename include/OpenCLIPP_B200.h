@@ -64,10 +64,12 @@ ocipError ocip_API ocipGetLaunchCount(uint64_t* Count);
  * The scan's scratch is a fixed 16 MiB array that every device which loads
  * the library holds until the process exits; images whose scratch would not
  * fit (about 7300 x 7300 pixels per channel) are refused with
- * CL_INVALID_IMAGE_SIZE. The first call on a device looks up that array's
- * device address; make that first call before capturing the stream into a
- * CUDA graph. All calls share the array: calls that overlap on the GPU (on
- * different streams, or on the same device from several threads) race. */
+ * CL_INVALID_IMAGE_SIZE. The first call in a CUDA context (on each device,
+ * and again after the device is reset) looks up that array's device address
+ * and may load the module; make that first call before capturing the stream
+ * into a CUDA graph. All calls share the array: calls that overlap on the GPU
+ * (on different streams, or on the same device from several threads) race,
+ * so the caller must serialise them. */
 ocipError ocip_API ocipIntegralNoAlloc(int Square, SImage SourceDesc, const void* Source,
                                        size_t SourcePitch, SImage DestDesc, void* Dest,
                                        size_t DestPitch, void* Stream);

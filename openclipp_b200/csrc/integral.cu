@@ -29,9 +29,11 @@
 //      ColTop at the last column of every tile left of x (LB at a tile's last
 //      column is the tile's total, so that sum is the integral of the tiles
 //      left of this one over the bands above).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -704,27 +706,69 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_noalloc_addr[kMaxDevices] = {};
+// Device addresses of g_noalloc_scratch, one per CUDA context that has used
+// it, keyed by the context's process-unique ID. A context that is destroyed
+// (cudaDeviceReset, or a primary context released and created again) loads
+// the module afresh, possibly at another address; its successor has a new
+// ID and therefore gets its own lookup, never a stale address.
+std::mutex g_noalloc_mutex;
+std::map<unsigned long long, void*> g_noalloc_addr;
 
-// The device address of g_noalloc_scratch on the current device. Host code
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+template <typename F>
+F driver_fn(const char* name) {
+  void* f = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &f, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(f);
+}
+
+// ID of the calling thread's current context, or false if there is none yet
+// (the runtime binds the device's primary context on its first real call).
+bool current_ctx_id(unsigned long long* id) {
+  static const CtxGetCurrentFn get_cur = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  CUcontext c = nullptr;
+  if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || c == nullptr) return false;
+  return get_id(c, id) == CUDA_SUCCESS;
+}
+
+// The device address of g_noalloc_scratch in the current context. Host code
 // cannot use the array's name as a device address; cudaGetSymbolAddress gives
-// the real one, once per device (on the first call made on that device).
-cudaError_t noalloc_scratch(int dev, void** ptr) {
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (g_noalloc_addr[dev] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_addr[dev] = p;
+// the real one. It is looked up once per context (the first call made in a
+// context, which may also load the module) and then served from the map.
+cudaError_t noalloc_scratch(void** ptr) {
+  unsigned long long id = 0;
+  bool have_id = current_ctx_id(&id);
+  if (have_id) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    auto it = g_noalloc_addr.find(id);
+    if (it != g_noalloc_addr.end()) {
+      *ptr = it->second;
+      return cudaSuccess;
+    }
   }
-  *ptr = g_noalloc_addr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  // The lookup made the primary context current if nothing was.
+  if (!have_id) have_id = current_ctx_id(&id);
+  if (have_id) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    g_noalloc_addr[id] = p;
+  }
+  *ptr = p;
   return cudaSuccess;
 }
 
 }  // namespace
 }  // namespace ocipb
 
+#include <climits>
 #include <string>
 
 #include "../../include/OpenCLIPP.h"
@@ -751,16 +795,19 @@ extern "C" ocipError ocipIntegralNoAlloc(int Square, SImage SourceDesc, const vo
     if (SourcePitch < (size_t)SourceDesc.Width * SourceDesc.Channels * type_bytes((int)SourceDesc.Type) ||
         DestPitch < (size_t)DestDesc.Width * DestDesc.Channels * type_bytes((int)DestDesc.Type))
       fail(CL_INVALID_VALUE, "pitch smaller than one row of pixels");
+    // Refused before the scratch size is computed in int arithmetic (a
+    // dimension above INT_MAX would wrap); far above the fixed limit anyway.
+    if (SourceDesc.Width > (unsigned)INT_MAX || SourceDesc.Height > (unsigned)INT_MAX)
+      fail(CL_INVALID_IMAGE_SIZE, "image too large for ocipIntegralNoAlloc: a dimension "
+                                  "exceeds INT_MAX, beyond the fixed scratch limit");
     const size_t need = integral_scratch_bytes((int)SourceDesc.Width, (int)SourceDesc.Height,
                                                (int)SourceDesc.Channels);
     if (need > kNoAllocScratchBytes)
       fail(CL_INVALID_IMAGE_SIZE,
            "image too large for ocipIntegralNoAlloc: needs " + std::to_string(need) +
                " bytes of scratch, the fixed limit is " + std::to_string(kNoAllocScratchBytes));
-    int dev = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     void* scratch = nullptr;
-    check_cuda(noalloc_scratch(dev, &scratch), "cudaGetSymbolAddress");
+    check_cuda(noalloc_scratch(&scratch), "cudaGetSymbolAddress");
     DevImage s, d;
     s.ptr = const_cast<void*>(Source);
     s.pitch = SourcePitch;
