@@ -65,13 +65,115 @@ def blob_field(W, H, nblobs=200, seed=0):
     return img.astype(np.float32)
 
 
-def workload(seed=0):
+def workload(seed=0, with_offset=False):
+    """The 4096x4096 F32 blob field and the 31x31 template cut from it at a
+    seeded offset (ty, tx); the exact match is output (tx + 15, ty + 15)."""
     S = blob_field(W_IMG, H_IMG, seed=seed)
     rng = np.random.default_rng(seed + 1)
     ty = int(rng.integers(0, H_IMG - T_SIDE))
     tx = int(rng.integers(0, W_IMG - T_SIDE))
     T = S[ty:ty + T_SIDE, tx:tx + T_SIDE].copy()
+    return (S, T, (ty, tx)) if with_offset else (S, T)
+
+
+def cfg1_images(seed=1):
+    """512x512 U8 uniform 0-255, 16x16 template cut at a seeded offset plus
+    round(N(0, 4^2)) noise, clipped to 0-255."""
+    rng = np.random.default_rng(seed)
+    S = rng.integers(0, 256, (512, 512), dtype=np.uint8)
+    y, x = (int(v) for v in rng.integers(0, 512 - 16, 2))
+    T = np.clip(S[y:y + 16, x:x + 16].astype(np.int32) + np.round(rng.normal(0, 4, (16, 16))),
+                0, 255).astype(np.uint8)
     return S, T
+
+
+def cfg5_images(dtype, seed=55):
+    """3840x2160x4 multi-channel field: uniform noise plus a blob field (U8),
+    or the blob field scaled to 0-65535 (U16); a 64x64x4 template cut at a
+    seeded offset. Returns (S, T, (y, x))."""
+    rng = np.random.default_rng(seed)
+    field = np.stack([blob_field(3840, 2160, nblobs=60, seed=seed + 5 + c) for c in range(4)], -1)
+    field = field / field.max()
+    if dtype == np.uint8:
+        S = np.clip(rng.integers(0, 128, field.shape) + 127 * field, 0, 255).astype(np.uint8)
+    else:
+        S = np.round(field * 65535).astype(np.uint16)
+    y, x = 700, 1900
+    return S, S[y:y + 64, x:x + 64].copy(), (y, x)
+
+
+# ---- accuracy against the FP64 / exact oracle ----------------------------------------
+
+def check_rows(H, th, n=256, match_row=None):
+    """n output rows spread over the valid region, the first and last rows of
+    the map, and the th rows around the match row (if given)."""
+    rows = set(np.linspace(th // 2, H - th + th // 2, n).astype(int).tolist())
+    rows |= {0, 1, H - 2, H - 1}
+    if match_row is not None:
+        rows |= set(range(max(0, match_row - th // 2), min(H, match_row + th // 2 + 1)))
+    return sorted(rows)
+
+
+def window_energy_rows(S, tw, th, rows):
+    """Sum of S^2 over each output's window (zero padding), FP64, for the
+    listed output rows: array (len(rows), W[, C])."""
+    sq = S.astype(np.float64) ** 2
+    H, W = S.shape[:2]
+    ax, ay = tw // 2, th // 2
+    pad = [(th, th), (tw, tw)] + ([(0, 0)] if S.ndim == 3 else [])
+    ii = np.pad(sq, pad).cumsum(0).cumsum(1)  # ii[i, j] = sum over [0, i] x [0, j] of padded
+    out = []
+    xs = np.arange(W)
+    for y in rows:
+        # window rows y - ay .. y - ay + th - 1, columns x - ax .. x - ax + tw - 1
+        r0, r1 = y - ay + th - 1, y - ay + 2 * th - 1  # padded index of the row before / last row
+        c0, c1 = xs - ax + tw - 1, xs - ax + 2 * tw - 1
+        out.append(ii[r1, c1] - ii[r0, c1] - ii[r1, c0] + ii[r0, c0])
+    return np.array(out)
+
+
+def scale_rows(measure, S, T, rows):
+    """The scale each measure's error is stated against, per output:
+    SqrDistance: sum S^2 + sum T^2 of the window (the terms that cancel to 0
+    at a match); CrossCorr: sum |S| |T| (equal to the value for non-negative
+    data; the bound of a dot product's rounding for signed data); the _Norm
+    forms divide these by sqrt(sum S^2 sum T^2); AbsDistance: its value."""
+    from oracle import oracle as O
+    th, tw = T.shape[:2]
+    es = window_energy_rows(S, tw, th, rows)
+    t64 = T.astype(np.float64)
+    et = (t64 ** 2).sum(axis=(0, 1))
+    if measure in (0, 1):
+        sc = es + et
+    elif measure in (3, 4):
+        sc = O.proximity_exact_rows(3, np.abs(S.astype(np.float64)), np.abs(t64), rows)
+    else:
+        return np.abs(O.proximity_exact_rows(2, S, T, rows))
+    if measure in (1, 4):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sc = sc / np.sqrt(es * et)
+    return sc
+
+
+def error_rows(measure, S, T, got, rows, ex=None):
+    """Errors of a computed map on the listed rows against the exact oracle:
+    max_abs, max_rel (per output, against |exact|), max_scaled (against the
+    measure's scale, scale_rows) and the share of outputs whose per-output
+    relative error is within 1e-5."""
+    from oracle import oracle as O
+    if ex is None:
+        ex = O.proximity_exact_rows(measure, S, T, rows)
+    g = got[rows].astype(np.float64)
+    sc = scale_rows(measure, S, T, rows)
+    fin = np.isfinite(ex) & np.isfinite(sc)
+    err = np.abs(g - ex)[fin]
+    ref = np.abs(ex[fin])
+    nz = ref > 0  # exact zeros (a perfect match) have no relative error
+    rel = err[nz] / ref[nz]
+    scaled = err / np.maximum(sc[fin], 1e-300)
+    return {"max_abs": float(err.max()), "max_rel": float(rel.max()) if rel.size else 0.0,
+            "max_scaled": float(scaled.max()),
+            "within_1e-5_rel": round(float((rel <= 1e-5).mean()), 6) if rel.size else 1.0}
 
 
 def valid_taps(W, H, tw, th, nch=1):
@@ -179,7 +281,7 @@ def run_ours(args, world, rank, local):
 
     from openclipp_b200 import ocip
 
-    S, T = workload(seed=1234 + rank)
+    S, T, (ty, tx) = workload(seed=1234 + rank, with_offset=True)
     H, W = S.shape
     MEASURES = args.measures
     taps_step = valid_taps(W, H, T_SIDE, T_SIDE) * len(MEASURES)
@@ -197,37 +299,26 @@ def run_ours(args, world, rank, local):
     Si.send()
     Ti.send()
 
-    def step():
-        for m, D in zip(MEASURES, Ds):
-            ocip.check(ocip.proximity(m, Si, Ti, D), m)
-
-    per_kernel = {}
-
-    def timed_steps(n, record=False):
+    def timed_steps(n, measures, record=None):
+        """n steps of `measures` (L2 flushed before each, not timed); per-measure
+        CUDA-event times go to `record` (a dict) when given."""
         times = []
         for _ in range(n):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            if record:
-                # per-measure events for the roofline of the dominant kernel
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(MEASURES) + 1)]
-                ev[0].record(stream)
-                for i, (m, D) in enumerate(zip(MEASURES, Ds)):
-                    ocip.check(ocip.proximity(m, Si, Ti, D), m)
-                    ev[i + 1].record(stream)
-            else:
-                step()
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-            if record:
-                for i, m in enumerate(MEASURES):
-                    per_kernel.setdefault(m, []).append(ev[i].elapsed_time(ev[i + 1]))
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(measures) + 1)]
+            ev[0].record(stream)
+            for i, m in enumerate(measures):
+                ocip.check(ocip.proximity(m, Si, Ti, Ds[MEASURES.index(m)]), m)
+                ev[i + 1].record(stream)
+            ev[-1].synchronize()
+            times.append(ev[0].elapsed_time(ev[-1]))
+            if record is not None:
+                for i, m in enumerate(measures):
+                    record.setdefault(m, []).append(ev[i].elapsed_time(ev[i + 1]))
         return times
 
-    timed_steps(args.warmup)
+    timed_steps(args.warmup, MEASURES)
     paths_used = {}
     for m, D in zip(MEASURES, Ds):
         ocip.check(ocip.proximity(m, Si, Ti, D), m)
@@ -235,17 +326,51 @@ def run_ours(args, world, rank, local):
     ctx.finish()
     torch.cuda.synchronize()
     barrier()
+    per_kernel = {}
     launches0 = ocip.launch_count()
     with Clocks(local) as clk:
-        times = timed_steps(args.steps, record=True)
+        times = timed_steps(args.steps, MEASURES, per_kernel)
     launches = ocip.launch_count() - launches0
     torch.cuda.synchronize()
     barrier()
     ms_step = allreduce_max(float(np.mean(times)))
     clocks = clk.summary()
 
-    # Accuracy of this run's maps against an FP64 oracle on a crop.
-    errs = accuracy_report(S, T, outs, Ds, MEASURES) if rank == 0 else {}
+    # Accuracy of this run's maps against the exact oracle on full rows
+    # (spread over the map, plus the template's rows around the match).
+    rows = check_rows(H, T_SIDE, n=256, match_row=ty + T_SIDE // 2)
+    acc = {}
+    if rank == 0 and not args.no_accuracy:
+        for D in Ds:
+            D.read()
+        acc[f"F32 {W}x{H} blob field, {T_SIDE}x{T_SIDE} ({args.path})"] = {
+            "rows": f"{len(rows)} full rows: 256 spread over the map, its first/last two, "
+                    f"rows {ty}-{ty + T_SIDE - 1} around the match",
+            **{m: dict(error_rows(MEAS_ALL.index(m), S, T, outs[i], rows), path=paths_used[m])
+               for i, m in enumerate(MEASURES)}}
+
+    # The metric's comparison: the plain FP32 kernels (the drop-in) on the
+    # same data, same step structure and L2 flush, for the product measures.
+    product = [m for m in MEASURES if m != "AbsDistance"]
+    per_kernel_plain = {}
+    if product and not args.no_plain_arm:
+        ctx.set_path(ocip.PATH_PLAIN)
+        timed_steps(3, product)
+        torch.cuda.synchronize()
+        barrier()
+        timed_steps(max(3, min(args.steps, 10)), product, per_kernel_plain)
+        torch.cuda.synchronize()
+        barrier()
+        if rank == 0 and not args.no_accuracy:
+            for m in product:
+                Ds[MEASURES.index(m)].read()
+            acc[f"F32 {W}x{H} blob field, {T_SIDE}x{T_SIDE} (plain FP32, reference arithmetic)"] = {
+                m: error_rows(MEAS_ALL.index(m), S, T, outs[MEASURES.index(m)], rows)
+                for m in product}
+        ctx.set_path(path)
+    if rank == 0 and not args.no_accuracy:
+        acc.update(accuracy_suite(ocip, ctx, S, (ty, tx), product))
+        ctx.set_path(path)
 
     # End-to-end arm: pinned host buffers, send + calls + reads per step.
     e2e_ms = run_e2e(args, ocip, torch, ctx, S, T, stream) if not args.no_e2e else float("nan")
@@ -259,6 +384,7 @@ def run_ours(args, world, rank, local):
     # remain in the step (AbsDistance has no product form) are reported beside
     # it against the FP32 ALU rate.
     med = {m: float(np.median(v)) for m, v in per_kernel.items()}
+    med_plain = {m: float(np.median(v)) for m, v in per_kernel_plain.items()}
     tensor_meas = [m for m in med if paths_used[m] == "tensor"] or list(med)
     dom = max(tensor_meas, key=med.get)
     peaks = load_peaks()
@@ -271,11 +397,7 @@ def run_ours(args, world, rank, local):
             "traffic": ncu_traffic(dom, paths_used[dom]),
             "peak_source": peaks["source"],
             "flops_convention": "2 per tap (one multiply-add), same-size map "
-                                f"{W}x{H}x{T_SIDE}x{T_SIDE} per launch",
-            "binding": "tcgen05.mma issue rate: one M=128, K=16 MMA per ~100 ns per SM for "
-                       "any N <= 256 (probe on this B200); F32 issues 3 split-BF16 products "
-                       "per tap and the Hankel operand pads K and N, so the tensor pipe does "
-                       "~3.9x the algorithmic flops and the flop fraction reads low"}
+                                f"{W}x{H}x{T_SIDE}x{T_SIDE} per launch"}
     plain_meas = [m for m in med if paths_used[m] == "plain"]
     roof_plain = {}
     for m in plain_meas:
@@ -298,7 +420,11 @@ def run_ours(args, world, rank, local):
                    "l2": "flushed before every step (256 MiB write, outside the timed events)"},
         "per_measure_ms": {m: round(v, 4) for m, v in med.items()},
         "per_measure_gtaps": {m: round(taps_meas / (v * 1e-3) / 1e9, 1) for m, v in med.items()},
-        "accuracy_vs_fp64": errs,
+        "tensor_per_measure_ms": {m: round(med[m], 4) for m in product if m in med},
+        "plain_per_measure_ms": {m: round(v, 4) for m, v in med_plain.items()},
+        "tensor_over_plain": {m: round(med_plain[m] / med[m], 2) for m in med_plain
+                              if paths_used.get(m) == "tensor"},
+        "accuracy_vs_fp64": acc,
         "roofline": roof,
         "roofline_plain": roof_plain,
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Gtaps/s",
@@ -315,6 +441,77 @@ def run_ours(args, world, rank, local):
     Ti.release()
     ctx.close()
     return result
+
+
+MEAS_ALL = ["SqrDistance", "SqrDistance_Norm", "AbsDistance", "CrossCorr", "CrossCorr_Norm"]
+
+
+def _run_maps(ocip, ctx, path, measures, S, T, out_dtype=np.float32):
+    """Each measure of (S, T) on the given path; returns {measure: map} and the
+    paths that served them."""
+    ctx.set_path(path)
+    Si, Ti = ocip.Image(S), ocip.Image(T)
+    maps, used = {}, {}
+    for m in measures:
+        out = np.zeros(S.shape, out_dtype)
+        D = ocip.Image(out)
+        ocip.check(ocip.proximity(m, Si, Ti, D), m)
+        D.read()
+        used[m] = {1: "plain", 2: "tensor"}[ctx.last_path()]
+        D.release()
+        maps[m] = out
+    Si.release()
+    Ti.release()
+    return maps, used
+
+
+def accuracy_suite(ocip, ctx, S, off, product):
+    """Error reports per measure and dtype beyond the timed workload:
+    the zero-mean (signed) variant of the 4096^2 F32 field on both paths,
+    the 512^2 U8 config (bit-exact count against the reference's own kernel
+    source), and the 3840x2160x4 U8/U16 config with a 64x64x4 template."""
+    from oracle import oracle as O
+    rep = {}
+    ty, tx = off
+    H, W = S.shape
+    rows = check_rows(H, T_SIDE, n=64, match_row=ty + T_SIDE // 2)
+    S0 = (S - np.float32(S.mean(dtype=np.float64))).astype(np.float32)
+    T0 = S0[ty:ty + T_SIDE, tx:tx + T_SIDE].copy()
+    for name, path in (("tensor", ocip.PATH_TENSOR), ("plain FP32, reference arithmetic",
+                                                      ocip.PATH_PLAIN)):
+        maps, used = _run_maps(ocip, ctx, path, product, S0, T0)
+        rep[f"F32 {W}x{H} zero-mean blob field, {T_SIDE}x{T_SIDE} ({name})"] = {
+            "rows": f"{len(rows)} full rows incl. the match's", "note":
+                "signed data: per-output relative error is unbounded where a sum cancels; "
+                "max_scaled states it against sum |S||T| (CrossCorr) or sum S^2 + sum T^2 "
+                "(SqrDistance), over sqrt(sum S^2 sum T^2) for _Norm",
+            **{m: dict(error_rows(MEAS_ALL.index(m), S0, T0, maps[m], rows), path=used[m])
+               for m in product}}
+    # 512x512 U8, 16x16 template: integer scores, bit-exact against the
+    # reference's own kernel source (built for the host).
+    S1, T1 = cfg1_images()
+    for name, path in (("tensor", ocip.PATH_TENSOR), ("plain", ocip.PATH_PLAIN)):
+        maps, used = _run_maps(ocip, ctx, path, MEAS_ALL[:], S1, T1)
+        r = {}
+        for m in MEAS_ALL:
+            want = (O.proximity_reference(m, S1, T1) if O.ref_available()
+                    else O.proximity_refexact(m, S1, T1))
+            r[m] = {"unequal_to_reference": int((~((maps[m] == want) |
+                                                   (np.isnan(maps[m]) & np.isnan(want)))).sum()),
+                    "outputs": int(want.size), "path": used[m]}
+        rep[f"U8 512x512, 16x16 ({name})"] = r
+    # 3840x2160x4 U8 and U16, 64x64x4 template, _Norm measures on the tensor path.
+    for dt, label in ((np.uint8, "U8"), (np.uint16, "U16")):
+        S5, T5, (y5, _) = cfg5_images(dt)
+        rows5 = sorted({0, 1, 2158, 2159, y5 + 32} |
+                       set(np.linspace(32, 2160 - 33, 6).astype(int).tolist()))
+        maps, used = _run_maps(ocip, ctx, ocip.PATH_TENSOR, ["SqrDistance_Norm", "CrossCorr_Norm"],
+                               S5, T5)
+        rep[f"{label} 3840x2160x4, 64x64x4 (tensor)"] = {
+            "rows": f"{len(rows5)} full rows (all 4 channels) incl. the match row",
+            **{m: dict(error_rows(MEAS_ALL.index(m), S5, T5, maps[m], rows5), path=used[m])
+               for m in maps}}
+    return rep
 
 
 def run_e2e(args, ocip, torch, ctx, S, T, stream):
@@ -351,24 +548,6 @@ def run_e2e(args, ocip, torch, ctx, S, T, stream):
     Si.release()
     Ti.release()
     return float(np.mean(times))
-
-
-def accuracy_report(S, T, outs, Ds, measures):
-    """Max abs / relative error of each map vs the FP64 oracle on a crop."""
-    from oracle import oracle as O
-    for D in Ds:
-        D.read()
-    y0, x0, n = 1000, 1000, 192
-    crop = S[y0 - 20:y0 + n + 20, x0 - 20:x0 + n + 20]
-    rep = {}
-    for i, m in enumerate(measures):
-        ex = O.proximity_exact(MEASURES.index(m), crop, T)[20:-20, 20:-20]
-        got = outs[i][y0:y0 + n, x0:x0 + n].astype(np.float64)
-        scale = np.abs(ex).max()
-        rel = np.abs(got - ex) / np.maximum(np.abs(ex), 1e-300)
-        rep[m] = {"max_abs": float(np.abs(got - ex).max()), "max_rel": float(rel.max()),
-                  "max_abs_over_maxref": float(np.abs(got - ex).max() / scale)}
-    return rep
 
 
 def ncu_traffic(measure, path):
@@ -959,6 +1138,10 @@ def main():
     ap.add_argument("--measures", default=",".join(MEASURES),
                     help="comma-separated subset of the five measures (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm (profiling)")
+    ap.add_argument("--no-plain-arm", action="store_true",
+                    help="skip timing the plain FP32 kernels beside the tensor path (profiling)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the error reports against the oracle (profiling)")
     ap.add_argument("--workload", choices=["single", "batch", "backward", "integral", "sad"],
                     default="single",
                     help="single: 4096^2 F32, 31x31, five measures (the headline); batch: 16 x "

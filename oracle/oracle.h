@@ -40,6 +40,13 @@ int orc_proximity_exact(int measure, int type, int nch, const void* src,
                         int src_step, const void* tmpl, int tmpl_step,
                         double* dst, int W, int H, int tw, int th);
 
+/* The same for the listed output rows only: dst is double[nrows][W*nch],
+ * row i holding output row rows[i]. */
+int orc_proximity_exact_rows(int measure, int type, int nch, const void* src,
+                             int src_step, const void* tmpl, int tmpl_step,
+                             double* dst, int W, int H, int tw, int th,
+                             const int* rows, int nrows);
+
 /* Window statistics of the same windows, exact: energy of the source window
  * (sum of squares, zero padding), cross term (sum S*T) and template energy.
  * Each array is double[H][W*nch]; tt is double[nch]. Any pointer may be NULL. */

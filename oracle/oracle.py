@@ -166,6 +166,24 @@ def proximity_exact(measure, src, tmpl):
     return out
 
 
+def proximity_exact_rows(measure, src, tmpl, rows):
+    """proximity_exact for the listed output rows only: float64 array of
+    shape (len(rows), W[, C]), row i holding output row rows[i]."""
+    lib = _lib_orc()
+    src, sp, ss, w, h, c = _img(src)
+    tmpl, tp, ts, tw, th, tc = _img(tmpl)
+    assert tc == c and tmpl.dtype == src.dtype
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    out = np.zeros((len(r), w, c) if src.ndim == 3 else (len(r), w), dtype=np.float64)
+    rc = lib.orc_proximity_exact_rows(measure_index(measure), type_index(src), c,
+                                      sp, ss, tp, ts,
+                                      out.ctypes.data_as(ctypes.c_void_p), w, h, tw, th,
+                                      r.ctypes.data_as(ctypes.c_void_p), len(r))
+    if rc:
+        raise RuntimeError(f"oracle returned {rc}")
+    return out
+
+
 def window_terms_exact(src, tmpl):
     """(sum S^2 per window, sum S*T per window, sum T^2 per channel)."""
     lib = _lib_orc()

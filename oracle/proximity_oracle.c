@@ -226,10 +226,12 @@ int orc_proximity_refexact(int measure, int type, int nch, const void* src,
 /* Exact window sums for integer sources: every product and sum in __int128. */
 static void exact_int(int measure, int type, int nch, const void* src, int ss,
                       const void* tmpl, int ts, double* dst, int W, int H,
-                      int tw, int th) {
+                      int tw, int th, const int* rows, int nrows) {
   const int left = -tw / 2, top = -th / 2;
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int gy = 0; gy < H; ++gy) {
+  const int n = rows ? nrows : H;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < n; ++i) {
+    const int gy = rows ? rows[i] : i;
     for (int gx = 0; gx < W; ++gx) {
       for (int c = 0; c < nch; ++c) {
         i128 sum = 0, sS = 0, sT = 0;
@@ -253,7 +255,7 @@ static void exact_int(int measure, int type, int nch, const void* src, int ss,
         long double v = (long double)sum;
         if (measure == 1 || measure == 4)
           v = v / sqrtl((long double)sS * (long double)sT);
-        dst[((size_t)gy * W + gx) * nch + c] = (double)v;
+        dst[((size_t)i * W + gx) * nch + c] = (double)v;
       }
     }
   }
@@ -263,10 +265,12 @@ static void exact_int(int measure, int type, int nch, const void* src, int ss,
  * values are exact in long double). */
 static void exact_flt(int measure, int type, int nch, const void* src, int ss,
                       const void* tmpl, int ts, double* dst, int W, int H,
-                      int tw, int th) {
+                      int tw, int th, const int* rows, int nrows) {
   const int left = -tw / 2, top = -th / 2;
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int gy = 0; gy < H; ++gy) {
+  const int n = rows ? nrows : H;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < n; ++i) {
+    const int gy = rows ? rows[i] : i;
     for (int gx = 0; gx < W; ++gx) {
       for (int c = 0; c < nch; ++c) {
         long double sum = 0, sS = 0, sT = 0;
@@ -288,7 +292,7 @@ static void exact_flt(int measure, int type, int nch, const void* src, int ss,
           }
         }
         if (measure == 1 || measure == 4) sum = sum / sqrtl(sS * sT);
-        dst[((size_t)gy * W + gx) * nch + c] = (double)sum;
+        dst[((size_t)i * W + gx) * nch + c] = (double)sum;
       }
     }
   }
@@ -301,10 +305,27 @@ int orc_proximity_exact(int measure, int type, int nch, const void* src,
   if (e) return e;
   if (type <= 5)
     exact_int(measure, type, nch, src, src_step, tmpl, tmpl_step, dst, W, H, tw,
-              th);
+              th, 0, 0);
   else
     exact_flt(measure, type, nch, src, src_step, tmpl, tmpl_step, dst, W, H, tw,
-              th);
+              th, 0, 0);
+  return 0;
+}
+
+int orc_proximity_exact_rows(int measure, int type, int nch, const void* src,
+                             int src_step, const void* tmpl, int tmpl_step,
+                             double* dst, int W, int H, int tw, int th,
+                             const int* rows, int nrows) {
+  int e = check_args(measure, type, nch, W, H, tw, th);
+  if (e) return e;
+  for (int i = 0; i < nrows; ++i)
+    if (rows[i] < 0 || rows[i] >= H) return -30;
+  if (type <= 5)
+    exact_int(measure, type, nch, src, src_step, tmpl, tmpl_step, dst, W, H, tw,
+              th, rows, nrows);
+  else
+    exact_flt(measure, type, nch, src, src_step, tmpl, tmpl_step, dst, W, H, tw,
+              th, rows, nrows);
   return 0;
 }
 

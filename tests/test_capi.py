@@ -131,3 +131,84 @@ def test_no_alloc_scratch_limit_is_checked_on_the_host(ocip):
                                           ctypes.c_void_p(16), w * 8, None)
         assert rc == ocip.CL_INVALID_IMAGE_SIZE, (w, h, rc)
         assert b"fixed limit" in ocip.lib.ocipGetLastErrorMessage()
+
+
+C_MATCHER = r'''
+/* A reference user's program: reads a U8 image and template from files,
+ * computes CrossCorr and SqrDistance_Norm through the drop-in header, and
+ * writes the score maps. */
+#include <stdio.h>
+#include <stdlib.h>
+#include "OpenCLIPP.h"
+#include "OpenCLIPP_B200.h"
+static int load(const char* path, void* buf, size_t n) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return 1;
+  size_t got = fread(buf, 1, n, f);
+  fclose(f);
+  return got != n;
+}
+int main(int argc, char** argv) {
+  const int W = 300, H = 200, TW = 21, TH = 17;
+  unsigned char* img = malloc(W * H);
+  unsigned char* tpl = malloc(TW * TH);
+  float* cc = malloc(sizeof(float) * W * H);
+  float* sqn = malloc(sizeof(float) * W * H);
+  if (argc < 5 || load(argv[1], img, W * H) || load(argv[2], tpl, TW * TH)) return 2;
+  ocipContext ctx = 0;
+  ocipError e = ocipInitialize(&ctx, NULL, CL_DEVICE_TYPE_GPU);
+  if (e != CL_SUCCESS) { printf("%s\n", ocipGetErrorName(e)); return 3; }
+  SImage si = {W, H, W, 1, U8}, st = {TW, TH, TW, 1, U8}, so = {W, H, W * 4, 1, F32};
+  ocipImage S, T, D1, D2;
+  ocipCreateImage(&S, si, img, CL_MEM_READ_WRITE);
+  ocipCreateImage(&T, st, tpl, CL_MEM_READ_WRITE);
+  ocipCreateImage(&D1, so, cc, CL_MEM_READ_WRITE);
+  ocipCreateImage(&D2, so, sqn, CL_MEM_READ_WRITE);
+  e = ocipCrossCorr(S, T, D1);
+  if (e == CL_SUCCESS) e = ocipSetProximityPath(OCIP_PATH_TENSOR);
+  if (e == CL_SUCCESS) e = ocipSqrDistance_Norm(S, T, D2);
+  if (e == CL_SUCCESS) e = ocipReadImage(D1);
+  if (e == CL_SUCCESS) e = ocipReadImage(D2);
+  printf("%s\n", ocipGetErrorName(e));
+  FILE* f = fopen(argv[3], "wb");
+  fwrite(cc, sizeof(float), W * H, f);
+  fclose(f);
+  f = fopen(argv[4], "wb");
+  fwrite(sqn, sizeof(float), W * H, f);
+  fclose(f);
+  ocipReleaseImage(S); ocipReleaseImage(T); ocipReleaseImage(D1); ocipReleaseImage(D2);
+  ocipUninitialize(ctx);
+  return e == CL_SUCCESS ? 0 : 1;
+}
+'''
+
+
+@pytest.mark.gpu
+def test_c_program_computes_maps_on_the_gpu():
+    """The C caller above, built against the headers and linked with
+    -lopenclipp_b200, computes a CrossCorr map (plain path) and a
+    SqrDistance_Norm map (tensor path) of a U8 image; both equal the exact
+    integer oracle rounded once (the sums stay below 2^24)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    rng = np.random.default_rng(12)
+    S = rng.integers(0, 256, (200, 300), dtype=np.uint8)
+    T = S[50:67, 100:121].copy()
+    with tempfile.TemporaryDirectory() as d:
+        c, exe = os.path.join(d, "matcher.c"), os.path.join(d, "matcher")
+        open(c, "w").write(C_MATCHER)
+        subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", INCLUDE, c, "-o", exe,
+                        "-L", LIBDIR, "-lopenclipp_b200", f"-Wl,-rpath,{LIBDIR}"],
+                       check=True, capture_output=True)
+        paths = [os.path.join(d, n) for n in ("S.bin", "T.bin", "cc.bin", "sqn.bin")]
+        S.tofile(paths[0])
+        T.tofile(paths[1])
+        r = subprocess.run([exe] + paths, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (r.stdout, r.stderr)
+        cc = np.fromfile(paths[2], np.float32).reshape(S.shape)
+        sqn = np.fromfile(paths[3], np.float32).reshape(S.shape)
+    assert np.array_equal(cc, O.proximity_exact(3, S, T).astype(np.float32))
+    ex = O.proximity_exact(1, S, T)
+    assert np.abs(sqn - ex).max() <= 1e-6 * np.abs(ex).max()
+    assert np.unravel_index(np.argmin(sqn), sqn.shape) == (50 + 8, 100 + 10)
