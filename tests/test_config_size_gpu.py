@@ -146,7 +146,17 @@ def test_cfg4_full_size_finite_differences_per_coordinate(ocip, ctx):
     FP64 central differences with h = 1e-3 at 32 image and 32 template
     coordinates. A perturbed pixel changes C and the window energies only
     where its windows reach, so L(+h) and L(-h) are evaluated exactly from the
-    FP64 maps updated there."""
+    FP64 maps updated there.
+
+    Bar, per coordinate: |g - fd| <= 1e-4 |fd| + 8 u sum|terms|, where
+    sum|terms| is the sum of the magnitudes of the terms the gradient adds up
+    and u = 2^-24 the FP32 rounding unit; and at least 60 of the 64
+    coordinates within 1e-4 relative alone. The second term matters only
+    where the gradient cancels: an image coordinate whose gradient is 1/2800
+    of its terms (kappa = sum|terms| / |g| = 2800) is below the resolution
+    of FP32 values of those terms at 1e-4, in any FP32 evaluation order (and
+    the FP64 central difference itself, with its O(h^2) truncation, is only
+    good to ~1e-4 there)."""
     ctx.make_current()
     ctx.set_path(ocip.PATH_TENSOR)
     rng = np.random.default_rng(4)
@@ -163,7 +173,7 @@ def test_cfg4_full_size_finite_differences_per_coordinate(ocip, ctx):
     g1, g2 = G1.astype(np.float64), G2.astype(np.float64)
     h = 1e-3
     ax, ay = tw // 2, th // 2
-    errs = []
+    rows = []  # (tensor, coordinate, fd, gpu, kappa)
     for _ in range(32):
         py, px = int(rng.integers(0, H)), int(rng.integers(0, W))
         # outputs whose window holds (px, py)
@@ -177,8 +187,13 @@ def test_cfg4_full_size_finite_differences_per_coordinate(ocip, ctx):
         Lp = _loss(G1l, G2l, c + h * tv, e + 2 * h * s + h * h, et)
         Lm = _loss(G1l, G2l, c - h * tv, e - 2 * h * s + h * h, et)
         fd = (Lp - Lm) / (2 * h)
-        errs.append(("S", py, px, abs(float(dS[py, px]) - fd) / abs(fd)))
+        # terms of dL/dS(p): 2 G1 (S(p) - T), G2 (T - N S(p) / E_S) / sqrt(E_S E_T)
+        q = np.sqrt(e * et)
+        mag = (np.abs(2 * G1l * s) + np.abs(2 * G1l * tv) + np.abs(G2l * tv / q) +
+               np.abs(G2l * (c / q) * s / e)).sum()
+        rows.append(("S", (py, px), fd, float(dS[py, px]), mag / abs(fd)))
     Sp = np.pad(S64, ((th, th), (tw, tw)))
+    q = np.sqrt(E * et)
     for _ in range(32):
         kh, kw = int(rng.integers(0, th)), int(rng.integers(0, tw))
         # C(x, y) gains h S(x + kw - ax, y + kh - ay) (zero outside)
@@ -187,9 +202,15 @@ def test_cfg4_full_size_finite_differences_per_coordinate(ocip, ctx):
         Lp = _loss(g1, g2, C + h * shift, E, et + 2 * h * t + h * h)
         Lm = _loss(g1, g2, C - h * shift, E, et - 2 * h * t + h * h)
         fd = (Lp - Lm) / (2 * h)
-        errs.append(("T", kh, kw, abs(float(dT[kh, kw]) - fd) / abs(fd)))
-    worst = max(errs, key=lambda r: r[3])
-    assert worst[3] <= 1e-4, worst
+        mag = (np.abs(2 * g1 * shift) + np.abs(2 * g1 * t) + np.abs(g2 * shift / q) +
+               np.abs(g2 * (C / q) * t / et)).sum()
+        rows.append(("T", (kh, kw), fd, float(dT[kh, kw]), mag / abs(fd)))
+    u = 2.0 ** -24
+    for name, coord, fd, g, kappa in rows:
+        err = abs(g - fd)
+        assert err <= 1e-4 * abs(fd) + 8 * u * kappa * abs(fd), (name, coord, fd, g, kappa)
+    within = sum(1 for r in rows if abs(r[3] - r[2]) <= 1e-4 * abs(r[2]))
+    assert within >= 60, f"only {within} of 64 coordinates within 1e-4 relative"
 
 
 def test_cfg5_u8_full_size_against_oracle(ocip, ctx):
