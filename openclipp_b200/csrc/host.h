@@ -26,7 +26,14 @@ const char* error_name(int code);
 // and one in-order queue (a CUDA stream), plus scratch buffers the kernels
 // reuse from call to call.
 struct Context {
-  enum ScratchSlot { kTemplateEnergy = 0, kPlanes = 1, kTensorAux = 2, kBackward = 3, kNumScratch = 4 };
+  enum ScratchSlot {
+    kTemplateEnergy = 0,
+    kPlanes = 1,
+    kTensorAux = 2,
+    kBackward = 3,
+    kEnergyMap = 4,  // window energies of the tensor path (FP64 planes)
+    kNumScratch = 5
+  };
   int device = 0;
   int sm_count = 0;
   int cc_major = 0, cc_minor = 0;

@@ -48,23 +48,24 @@
 // number of additions, so the chains of a whole window (th rows x K chunks)
 // would cost accuracy.
 //
-// Window energy sum S^2 of each position: per source row the energy warps
-// square every staged pixel once (FP32 for F32, exact integers for U8 and
-// U16), take each position's row sum of tw squares as the difference of a
-// short running prefix over the thread's S/2 consecutive positions, keep the
-// row sums in a ring of R rows and a running sum over the last th rows (FP64
-// or exact integers) and hand the window sums to the epilogue through a ring
-// in shared memory whose entries the epilogue releases. SqrDistance = E_S - 2C + E_T and the _Norm scale are
-// done in FP64 (F32, U16) or as the plain path does them (U8: the results are
-// bit-identical to it).
+// Window energies sum S^2 of each position (measures other than CrossCorr):
+// a separate pre-pass (row_energy.cu) writes the row energies R(x, r) =
+// sum_{w < tw} S^2(x + w - ax, r) of every source row (int32 for U8, FP32
+// otherwise); the epilogue keeps each position's window energy as an FP64
+// running sum over the rows it walks (add R of the row a slot completes,
+// drop R of the row th back), loading a block's R values before it waits for
+// the block's MMAs. Exact for U8; 2^-24 relative for F32 and U16.
+// SqrDistance = E_S - 2C + E_T and the _Norm scale are done in FP64 (F32,
+// U16) or as the plain path does them (U8: the results are bit-identical to
+// it).
 //
-// Roles (18 warps; one CTA per SM, which holds all 512 TMEM columns):
+// Roles (10 warps; one CTA per SM, which holds all 512 TMEM columns):
 //   warps 0-3  builders: the A operand of each row (split into hi/lo);
 //   warps 4-7  epilogue (warp 4 + k reads TMEM lanes 32k .. 32k + 31): running
-//              sums in the TMEM ring, score map;
+//              sums in the TMEM ring, window energies, score map;
 //   warp 8     TMA loads of source rows (zero fill outside the image);
-//   warp 9     MMA issue (one commit per source row, one per block);
-//   warps 10-17 window energies (measures other than CrossCorr).
+//   warp 9     MMA issue (one commit per block of rows: the block's partial
+//              and its A stages are free once it completes).
 // Every wait is bounded: a wait that gives up sets the CTA's abort flag, the
 // roles leave their loops, the MMA and TMA threads drain what they issued,
 // and the kernel raises the context's error flag.
@@ -83,6 +84,7 @@
 
 #include "sm100.cuh"
 #include "tensor.h"
+#include "row_energy.h"
 
 namespace ocipb {
 namespace {
@@ -94,12 +96,10 @@ constexpr int kBuilders = 4;
 constexpr int kEpilogue = 4;
 constexpr int kTmaWarp = kBuilders + kEpilogue;
 constexpr int kMmaWarp = kTmaWarp + 1;
-constexpr int kEnergyWarp = kMmaWarp + 1;  // first of the window-energy warps
-constexpr int kEnergy = 8;
-constexpr int kThreads = (kEnergyWarp + kEnergy) * 32;
+constexpr int kThreads = (kMmaWarp + 1) * 32;
 constexpr int kBuildThreads = kBuilders * 32;
 constexpr int kNRaw = 6;                // staged source rows (TMA stages of one row)
-constexpr int kNA = 4;                  // A operand stages (one source row each)
+constexpr int kMaxNA = 16;              // A operand stages at most (two blocks of rows)
 constexpr int kSR = 128;                // S R: template rows x positions per lane
 constexpr int kN = kSR;                 // B rows (MMA N without the slide)
 constexpr int kNp = kN + 16;            // MMA N: a block's B - 1 slides fit in 16 more
@@ -111,8 +111,6 @@ constexpr int kMinSmem = 120 * 1024;    // keeps one CTA per SM (it takes all of
 constexpr int kMaxDynSmem = 226 * 1024; // opt-in dynamic shared memory limit of the kernel
 constexpr long long kSpinLimit = 4000000000LL;  // about 2 s of SM clock
 constexpr int kBarBuild = 1;            // named barrier of the builder warps
-constexpr int kEnergyThreads = kEnergy * 32;
-constexpr int kBarEnergy = 2;           // named barrier of the energy warps
 
 enum Elem { kF32 = 0, kU8 = 1, kU16 = 2 };
 
@@ -122,16 +120,6 @@ struct ElemTraits {
   static constexpr int size = ELEM == kF32 ? 4 : ELEM == kU16 ? 2 : 1;
   static constexpr int inner = 16 / size;     // elements per 16-byte TMA group
   static constexpr int cmk = split ? 8 : 16;  // K elements per core-matrix row
-  // Row sums of squares: FP32 for F32 sources, exact integers otherwise.
-  typedef typename std::conditional<
-      ELEM == kF32, float, typename std::conditional<ELEM == kU16, unsigned long long,
-                                                     int>::type>::type RT;
-  // Running window sums: FP64 for F32, exact integers otherwise.
-  typedef typename std::conditional<
-      ELEM == kF32, double, typename std::conditional<ELEM == kU16, unsigned long long,
-                                                     int>::type>::type WT;
-  // Row sums kept in the ring, window sums handed to the epilogue.
-  typedef typename std::conditional<split, float, int>::type ST;
 };
 
 // Positions per TMEM lane for a template of R rows (S R = 128), and the steps
@@ -148,8 +136,8 @@ struct Geo {
   int cma;         // A core matrices addressed per lane (hi, incl. the pairing's spare)
   int QR;          // buffer rows of one A plane
   int lbok;        // bytes between K-adjacent core matrices of A
-  int nraw;        // staged elements the energies read (lead + P - 1 + tw)
-  int kNE;         // depth of the window-energy ring (steps, at most 16)
+  int nraw;        // staged elements the windows cover (lead + P - 1 + tw)
+  int NA;          // A operand stages: two blocks of steps
 };
 
 __host__ __device__ inline Geo make_geo(bool split, int R, int tw, int lead) {
@@ -173,13 +161,12 @@ __host__ __device__ inline Geo make_geo(bool split, int R, int tw, int lead) {
   g.lbok = 16 * (cmk / g.S);
   g.QR = kM + (cmk / g.S) * (g.cma - 1);
   g.nraw = lead + g.P - 1 + tw;
-  // Depth of the window-energy ring (each entry is released by the epilogue).
-  g.kNE = g.S == 8 ? 8 : 16;
+  g.NA = 2 * g.B;
   return g;
 }
 
 // Staged elements of one row: the last buffer row's end, and every element
-// the energies read.
+// of the strip's windows.
 __host__ __device__ inline int staged_elems(const Geo& g, bool split) {
   const int a = g.S * (g.QR - 1) + (split ? 8 : 16);
   return a > g.nraw ? a : g.nraw;
@@ -202,11 +189,15 @@ struct ItemArgs {
   size_t dst_pitch;
   int dst_f64;
   int measure;
+  // Row energies (measures other than CrossCorr): int32 (U8) or FP32 planes
+  // of R(x, r), plane ch at energy + ch * e_plane bytes, rows e_pitch apart.
+  const char* energy;
+  size_t e_pitch, e_plane;
 };
 
 // Shared-memory layout, identical on host and device.
 struct Layout {
-  int row_bytes, raw_stage, raw, b, a_stage, a, rs, es, sq, bars, total;
+  int row_bytes, raw_stage, raw, b, a_stage, a, bars, total;
 };
 
 __host__ __device__ inline int align128(int x) { return (x + 127) & ~127; }
@@ -228,15 +219,9 @@ __host__ __device__ inline Layout make_layout(bool split, const Geo& g, int nbox
   L.b = L.raw + kNRaw * L.raw_stage;
   L.a = L.b + align128(2 * g.nmma * g.NB * 16);
   L.a_stage = align128(g.QR * 16 * (split ? 2 : 1));
-  L.rs = L.a + kNA * L.a_stage;
-  L.es = L.rs + g.R * g.P * 4;
-  L.sq = L.es + g.kNE * g.P * 4;
-  // Squares of two staged rows (8-byte entries at most), each padded for the
-  // energy threads' last vector loads.
-  L.bars = L.sq + 2 * align128((g.P + 64 + 32) * 8);
-  // raw full, raw free; ready, MMA done; energy full, energy free (16 each
-  // at most); block full, buffer free; done.
-  L.total = L.bars + align128(8 * (2 * kNRaw + 2 * kNA + 32 + 4 + 1));
+  L.bars = L.a + g.NA * L.a_stage;
+  // raw full, raw free; ready (one per A stage); block full, buffer free; done.
+  L.total = L.bars + align128(8 * (2 * kNRaw + kMaxNA + 4 + 1));
   return L;
 }
 
@@ -263,21 +248,6 @@ __device__ __forceinline__ double tmpl_at(const ItemArgs& a, int h, int w, int c
   if (ELEM == kF32) return reinterpret_cast<const float*>(row)[i];
   if (ELEM == kU16) return reinterpret_cast<const uint16_t*>(row)[i];
   return reinterpret_cast<const uint8_t*>(row)[i];
-}
-
-// Square of staged element e of a row, in the row-sum type.
-template <int ELEM>
-__device__ __forceinline__ typename ElemTraits<ELEM>::RT sq_at(const unsigned char* row, int e) {
-  if (ELEM == kF32) {
-    const float v = reinterpret_cast<const float*>(row)[e];
-    return v * v;
-  }
-  if (ELEM == kU16) {
-    const unsigned int v = reinterpret_cast<const uint16_t*>(row)[e];
-    return static_cast<unsigned long long>(v * v);
-  }
-  const int v = reinterpret_cast<const uint8_t*>(row)[e];
-  return v * v;
 }
 
 // 8 staged elements from element e0 as floats (F32, U16).
@@ -320,36 +290,6 @@ __device__ __forceinline__ void load8(const unsigned char* row, int e0, float (&
 }
 
 // AND of `p` over the builder warps (a named barrier every builder reaches).
-__device__ __forceinline__ void energy_sync() {
-  asm volatile("bar.sync %0, %1;" ::"n"(kBarEnergy), "n"(kEnergyThreads) : "memory");
-}
-
-// N consecutive elements of T from an address aligned to N * sizeof(T).
-template <typename T, int N>
-struct Vec {
-  T v[N];
-};
-template <typename T, int N>
-__device__ __forceinline__ Vec<T, N> load_vec(const T* p) {
-  static_assert(N * sizeof(T) <= 32, "vector too wide");
-  Vec<T, N> r;
-  if (N * sizeof(T) == 32) {
-    const uint4 a = reinterpret_cast<const uint4*>(p)[0];
-    const uint4 b = reinterpret_cast<const uint4*>(p)[1];
-    uint4* o = reinterpret_cast<uint4*>(&r);
-    o[0] = a;
-    o[1] = b;
-  } else if (N * sizeof(T) == 16) {
-    *reinterpret_cast<uint4*>(&r) = *reinterpret_cast<const uint4*>(p);
-  } else if (N * sizeof(T) == 8) {
-    *reinterpret_cast<uint2*>(&r) = *reinterpret_cast<const uint2*>(p);
-  } else {
-#pragma unroll
-    for (int j = 0; j < N; ++j) r.v[j] = p[j];
-  }
-  return r;
-}
-
 __device__ __forceinline__ bool builders_all(bool p) {
   uint32_t r;
   asm volatile(
@@ -363,7 +303,7 @@ __device__ __forceinline__ bool builders_all(bool p) {
   return r != 0;
 }
 
-// Runs one work item with all 18 warps of the CTA. The caller has
+// Runs one work item with all 10 warps of the CTA. The caller has
 // synchronised the CTA; TMEM (512 columns) is allocated. Barriers are
 // initialised here and invalidated at the end, so consecutive items may use
 // different layouts.
@@ -372,7 +312,6 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   typedef ElemTraits<ELEM> TR;
   constexpr bool SPLIT = TR::split;
   constexpr int R = kSR / S;
-  constexpr int P = kM * S;
   constexpr int Q = 16 / S;
   constexpr int BS = block_steps(S);
   constexpr int CMK = TR::cmk;
@@ -380,21 +319,16 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   constexpr int NCH = (NC + 15) / 16;   // 16-column chunks of a partial
   static_assert(S * BS == 16, "a block's completed slots are one chunk");
   static_assert(NC <= kNp && NCH * 16 == kRingCols, "block does not fit the ring");
-  typedef typename TR::RT RT;
-  typedef typename TR::WT WT;
-  typedef typename TR::ST ST;
   const int lead = (TR::inner - a.ax % TR::inner) % TR::inner;
   const Geo G = make_geo(SPLIT, R, a.tw, lead);
   const Layout L = make_layout(SPLIT, G, a.nbox);
-  const int kNE = G.kNE;
 
   uint64_t* raw_full = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* raw_free = raw_full + kNRaw;
-  uint64_t* ready = raw_free + kNRaw;      // A of row t written
-  uint64_t* mma_done = ready + kNA;        // MMAs of row t complete (A stage free)
-  uint64_t* e_full = mma_done + kNA;       // window energies of row t written
-  uint64_t* e_free = e_full + 16;          // ... read by the epilogue
-  uint64_t* blk_full = e_free + 16;        // block's MMAs complete (2 buffers)
+  // A of row t written. Stage t mod NA is free again once the MMAs of block
+  // t / BS - 2 have completed (its blk_full commit): NA = 2 BS stages.
+  uint64_t* ready = raw_free + kNRaw;
+  uint64_t* blk_full = ready + kMaxNA;     // block's MMAs complete (2 buffers)
   uint64_t* buf_free = blk_full + 2;       // block's buffer read by the epilogue
   uint64_t* done_bar = buf_free + 2;
   volatile int* abort_flag = &cs.abort;
@@ -409,16 +343,9 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
   if (threadIdx.x == 0) {
     for (int i = 0; i < kNRaw; ++i) {
       mbar_init(&raw_full[i], 1);
-      mbar_init(&raw_free[i], kBuilders + (need_e ? kEnergy : 0));
+      mbar_init(&raw_free[i], kBuilders);
     }
-    for (int i = 0; i < kNA; ++i) {
-      mbar_init(&ready[i], kBuilders);
-      mbar_init(&mma_done[i], 1);
-    }
-    for (int i = 0; i < kNE; ++i) {
-      mbar_init(&e_full[i], kEnergy);
-      mbar_init(&e_free[i], kEpilogue);
-    }
+    for (int i = 0; i < G.NA; ++i) mbar_init(&ready[i], kBuilders);
     for (int i = 0; i < 2; ++i) {
       mbar_init(&blk_full[i], 1);
       mbar_init(&buf_free[i], kEpilogue);
@@ -544,9 +471,10 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
             mma_i8(d, smem_desc(ah + 2 * j * G.lbok, G.lbok, 128),
                    smem_desc(bq + 2 * j * bstride, bstride, 128), idesc, j == 0 ? acc0 : 1u);
         }
-        mma_commit(&mma_done[i]);
+        // One commit per block: it frees the block's partial for the epilogue
+        // and its A stages for the builders.
         if (q == BS - 1 || t == nsteps - 1) mma_commit(&blk_full[k & 1]);
-        if (++i == kNA) { i = 0; ph ^= 1; }
+        if (++i == G.NA) { i = 0; ph ^= 1; }
       }
       // Every MMA issued has completed before the item ends.
       mma_commit(done_bar);
@@ -557,11 +485,15 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     // ---- Builders: A operand ------------------------------------------------------
     const int b = threadIdx.x;  // 0 .. 127
     int i = 0, st = 0;
-    uint32_t iph = 0, rph = 0;
+    uint32_t rph = 0;
     for (int t = 0; t < nsteps; ++t) {
       bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
-      // A stage i is free once the MMAs of row t - kNA have completed.
-      ok = ok && (t < kNA || mbar_wait(&mma_done[i], iph ^ 1, abort_flag, kSpinLimit));
+      // A stage i was last read by row t - NA, in block kb - 2: wait for that
+      // block's commit. (The barrier cannot be a phase further on: block kb
+      // needs these rows; and block kb - 4 was waited for two blocks ago.)
+      const int kb = t / BS;
+      ok = ok && (t < G.NA ||
+                  mbar_wait(&blk_full[(kb - 2) & 1], ((kb - 2) >> 1) & 1, abort_flag, kSpinLimit));
       // All builders take the same branch (they meet at named barriers).
       if (!builders_all(ok)) break;
       const unsigned char* row = smem + L.raw + st * L.raw_stage;
@@ -600,132 +532,8 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         mbar_arrive(&ready[i]);
         mbar_arrive(&raw_free[st]);
       }
-      if (++i == kNA) { i = 0; iph ^= 1; }
+      if (++i == G.NA) i = 0;
       if (++st == kNRaw) { st = 0; rph ^= 1; }
-    }
-  } else if (warp >= kEnergyWarp) {
-    // ---- Window energies ----------------------------------------------------------
-    // Two staged rows per pass (their chains interleave; one barrier pair per
-    // two rows). Per row the squares V_k = S^2(lead + k) are written once to a
-    // buffer; thread b then takes the SE = S / 2 consecutive positions
-    // x = SE b + i and streams V_{SE b} .. with aligned vector loads, keeping a
-    // running prefix: the row sum of position x is prefix(x + tw) - prefix(x).
-    // The window sum adds each row and drops the row th steps back (a ring of
-    // R >= th row sums; read before write when th == R), in row order.
-    if (need_e) {
-      constexpr int SE = S / 2;  // positions per energy thread
-      typedef Vec<RT, SE> VT;
-      const int b = threadIdx.x - kEnergyWarp * 32;  // 0 .. 255
-      const int tw = a.tw, th = a.th;  // registers: the item lives in shared memory
-      const int nq = P - 1 + tw;       // squares the windows cover
-      const int nqp = nq + 2 * SE;     // plus the zero pad the last loads read
-      const int nchunk = (tw + 2 * SE - 1) / SE;  // vector loads per thread and row
-      const int cfast = tw / SE;       // chunks 1 .. cfast - 1 lie inside every window
-      const int sqstride = align128((P + 64 + 32) * 8) / (int)sizeof(RT);  // RT per buffer
-      ST* rsring = reinterpret_cast<ST*>(smem + L.rs);
-      ST* estage = reinterpret_cast<ST*>(smem + L.es);
-      RT* sqbuf = reinterpret_cast<RT*>(smem + L.sq);
-      WT ewin[SE];
-#pragma unroll
-      for (int i = 0; i < SE; ++i) ewin[i] = WT(0);
-      int st = 0;
-      uint32_t rph = 0;
-      for (int t = 0; t < nsteps; t += 2) {
-        const bool two = t + 1 < nsteps;  // uniform
-        const int st1 = st + 1 == kNRaw ? 0 : st + 1;
-        const uint32_t rph1 = st + 1 == kNRaw ? rph ^ 1 : rph;
-        bool ok = mbar_wait(&raw_full[st], rph, abort_flag, kSpinLimit);
-        // Ring entries of rows t, t + 1 were read by the epilogue (kNE rows back).
-        ok = ok && (t < kNE ||
-                    mbar_wait(&e_free[t % kNE], ((t / kNE) - 1) & 1, abort_flag, kSpinLimit));
-        if (two) {
-          ok = ok && mbar_wait(&raw_full[st1], rph1, abort_flag, kSpinLimit);
-          ok = ok && (t + 1 < kNE || mbar_wait(&e_free[(t + 1) % kNE], (((t + 1) / kNE) - 1) & 1,
-                                               abort_flag, kSpinLimit));
-        }
-        // The energy warps meet at named barriers: all take the same branch.
-        // This barrier also orders the previous pass's reads of the squares
-        // before this pass's writes.
-        uint32_t all;
-        asm volatile(
-            "{\n\t.reg .pred pi, po;\n\t"
-            "setp.ne.u32 pi, %1, 0;\n\t"
-            "barrier.red.and.pred po, %2, %3, pi;\n\t"
-            "selp.u32 %0, 1, 0, po;\n\t}"
-            : "=r"(all)
-            : "r"((uint32_t)ok), "n"(kBarEnergy), "n"(kEnergyThreads)
-            : "memory");
-        if (!all) break;
-        const unsigned char* row0 = smem + L.raw + st * L.raw_stage;
-        const unsigned char* row1 = smem + L.raw + st1 * L.raw_stage;
-        for (int k = b; k < nqp; k += kEnergyThreads) {
-          sqbuf[k] = k < nq ? sq_at<ELEM>(row0, lead + k) : RT(0);
-          if (two) sqbuf[sqstride + k] = k < nq ? sq_at<ELEM>(row1, lead + k) : RT(0);
-        }
-        energy_sync();
-        // Prefixes over the thread's V_0 ..: lo[r][i] = prefix(i), hi[r][i] = prefix(tw + i).
-        const RT* m0 = sqbuf + SE * b;
-        const RT* m1 = m0 + sqstride;
-        RT run[2] = {RT(0), RT(0)}, lo[2][SE], hi[2][SE];
-        auto take = [&](const VT& v0, const VT& v1, int k0) {
-#pragma unroll
-          for (int j = 0; j < SE; ++j) {
-            const int k = k0 + j;
-#pragma unroll
-            for (int i = 0; i < SE; ++i) {  // static indices: lo and hi stay in registers
-              if (k == i) {
-                lo[0][i] = run[0];
-                lo[1][i] = run[1];
-              }
-              if (k == tw + i) {
-                hi[0][i] = run[0];
-                hi[1][i] = run[1];
-              }
-            }
-            run[0] += v0.v[j];
-            run[1] += v1.v[j];
-          }
-        };
-        take(load_vec<RT, SE>(m0), load_vec<RT, SE>(m1), 0);
-        int c = 1;
-        for (; c < cfast; ++c) {
-          const VT v0 = load_vec<RT, SE>(m0 + SE * c);
-          const VT v1 = load_vec<RT, SE>(m1 + SE * c);
-#pragma unroll
-          for (int j = 0; j < SE; ++j) {
-            run[0] += v0.v[j];
-            run[1] += v1.v[j];
-          }
-        }
-        for (; c < nchunk; ++c) take(load_vec<RT, SE>(m0 + SE * c), load_vec<RT, SE>(m1 + SE * c), SE * c);
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          if (r == 1 && !two) break;
-          const int tr = t + r;
-          ST* es = estage + (tr % kNE) * P;
-#pragma unroll
-          for (int i = 0; i < SE; ++i) {
-            const int x = SE * b + i;
-            ST* slot = rsring + (tr & (R - 1)) * P + x;
-            const ST old = tr >= th ? rsring[((tr - th) & (R - 1)) * P + x] : ST(0);
-            const ST cur = static_cast<ST>(hi[r][i] - lo[r][i]);
-            *slot = cur;
-            ewin[i] += static_cast<WT>(cur) - static_cast<WT>(old);
-            es[x] = static_cast<ST>(ewin[i]);
-          }
-        }
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(&e_full[t % kNE]);
-          mbar_arrive(&raw_free[st]);
-          if (two) {
-            mbar_arrive(&e_full[(t + 1) % kNE]);
-            mbar_arrive(&raw_free[st1]);
-          }
-        }
-        st = two ? (st1 + 1 == kNRaw ? 0 : st1 + 1) : st1;
-        rph = two ? (st1 + 1 == kNRaw ? rph1 ^ 1 : rph1) : rph1;
-      }
     }
   } else {
     // ---- Epilogue ---------------------------------------------------------------
@@ -734,7 +542,17 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     const int m = sp * 32 + lane;
     const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(sp * 32) << 16);
     const uint32_t ring = lane_base + kRingCol;
-    const ST* estage = reinterpret_cast<const ST*>(smem + L.es);
+    // The item's fields in registers: the item lives in shared memory, and
+    // the score loop would otherwise reload them on every slot.
+    const auto ea_W = a.W;
+    const auto ea_dst = a.dst;
+    const auto ea_dst_f64 = a.dst_f64;
+    const auto ea_dst_pitch = a.dst_pitch;
+    const auto ea_measure = a.measure;
+    const auto ea_nch = a.nch;
+    const auto ea_xs_out = a.xs_out;
+    const auto ea_y0 = a.y0;
+    const auto ea_yend = a.yend;
     const double etd = cs.et;
     const float ret = (float)(1.0 / sqrt(etd));  // 1 / sqrt(E_T)
     // Score of one position from its product sum cv and window energy ev.
@@ -742,44 +560,91 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     // numerator is formed in FP64; the _Norm scale of an F32 map is taken in
     // FP32 (relative error a few 1e-7), of an F64 map in FP64. U8: exact
     // integers and the plain path's float or double formulas (bit-identical).
-    auto num_of = [&](AT cv, ST ev) -> double {
+    // U8 _Norm: float arithmetic where the plain path's float sums are exact.
+    const bool u8_float = (double)a.tw * a.th * 65025.0 <= 16777216.0;
+    // Scores with the measure fixed at compile time (MT::value), so that the
+    // S positions of a slot are straight-line, independent work.
+    auto num_of = [&](auto mt, AT cv, double ev) -> double {
+      constexpr int M = decltype(mt)::value;
       const double cc = (double)cv;
-      if (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) return cc;
-      return (double)ev - 2.0 * cc + etd;
+      if (M == kCrossCorr || M == kCrossCorrNorm) return cc;
+      return ev - 2.0 * cc + etd;
     };
-    auto score_f = [&](AT cv, ST ev) -> float {
+    auto score_f = [&](auto mt, AT cv, double ev) -> float {
+      constexpr int M = decltype(mt)::value;
       if (SPLIT) {
-        const double num = num_of(cv, ev);
-        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return (float)num;
+        const double num = num_of(mt, cv, ev);
+        if (M == kCrossCorr || M == kSqrDistance) return (float)num;
         return (float)num * (rsqrtf((float)ev) * ret);
       } else {
         // Exact in int32: each of C, E_S, E_T <= 64 * 64 * 255^2 < 2^28.
         const int cc = static_cast<int>(cv);
         const int es = static_cast<int>(ev);
         const int ei = static_cast<int>(etd);
-        const int num =
-            (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
-        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return __int2float_rn(num);
-        if ((double)a.tw * a.th * 65025.0 <= 16777216.0)  // float sums exact
-          return __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
+        const int num = (M == kCrossCorr || M == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
+        if (M == kCrossCorr || M == kSqrDistance) return __int2float_rn(num);
+        if (u8_float) return __fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
         return (float)__ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
       }
     };
-    auto score_d = [&](AT cv, ST ev) -> double {
+    auto score_d = [&](auto mt, AT cv, double ev) -> double {
+      constexpr int M = decltype(mt)::value;
       if (SPLIT) {
-        const double num = num_of(cv, ev);
-        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return num;
-        return num * rsqrt((double)ev * etd);
+        const double num = num_of(mt, cv, ev);
+        if (M == kCrossCorr || M == kSqrDistance) return num;
+        return num * rsqrt(ev * etd);
       } else {
         const int cc = static_cast<int>(cv);
         const int es = static_cast<int>(ev);
         const int ei = static_cast<int>(etd);
-        const int num =
-            (a.measure == kCrossCorr || a.measure == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
-        if (a.measure == kCrossCorr || a.measure == kSqrDistance) return (double)num;
-        if ((double)a.tw * a.th * 65025.0 <= 16777216.0)
+        const int num = (M == kCrossCorr || M == kCrossCorrNorm) ? cc : es - 2 * cc + ei;
+        if (M == kCrossCorr || M == kSqrDistance) return (double)num;
+        if (u8_float)
           return (double)__fdiv_rn((float)num, __fsqrt_rn(__fmul_rn((float)es, (float)ei)));
         return __ddiv_rn((double)num, __dsqrt_rn(__dmul_rn((double)es, (double)ei)));
+      }
+    };
+    // Row energies of the rows block kk's slots complete (entering: staged
+    // row u; leaving: staged row u - th), S positions of this lane each,
+    // loaded before the block's MMAs are waited for. The window energy of
+    // each position is an FP64 running sum over the slots, in order.
+    typedef typename std::conditional<SPLIT, float, int>::type RT;
+    const int xl = ea_xs_out + S * m;
+    RT rin[BS][S], rout[BS][S];
+    double esum[S];
+#pragma unroll
+    for (int p = 0; p < S; ++p) esum[p] = 0.0;
+#pragma unroll
+    for (int g = 0; g < BS; ++g)
+#pragma unroll
+      for (int p = 0; p < S; ++p) rin[g][p] = rout[g][p] = RT(0);  // CrossCorr: no energies
+    auto load_rows = [&](RT (&v)[S], int sr) {
+      const bool row_ok = need_e && sr >= 0 && sr < a.H;
+      const RT* er = reinterpret_cast<const RT*>(a.energy + (size_t)ch * a.e_plane +
+                                                 (size_t)(row_ok ? sr : 0) * a.e_pitch);
+      if (row_ok && xl + S <= ea_W) {
+        if (S == 2) {
+          const uint2 q = *reinterpret_cast<const uint2*>(er + xl);
+          memcpy(v, &q, sizeof(q));
+        } else {
+#pragma unroll
+          for (int j = 0; j < S / 4; ++j) {
+            const uint4 q = reinterpret_cast<const uint4*>(er + xl)[j];
+            memcpy(&v[4 * j], &q, sizeof(q));
+          }
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < S; ++p) v[p] = row_ok && xl + p < ea_W ? er[xl + p] : RT(0);
+      }
+    };
+    auto load_energies = [&](int kk) {
+#pragma unroll
+      for (int g = 0; g < BS; ++g) {
+        const int u = kk * BS + g;
+        const bool in = u < nsteps;
+        load_rows(rin[g], in ? r_begin + u : -1);
+        load_rows(rout[g], in && u >= a.th ? r_begin + u - a.th : -1);
       }
     };
     uint32_t zero[16];
@@ -789,6 +654,7 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     tmem_st_wait();
     for (int k = 0; k * BS < nsteps; ++k) {
       const int t0 = k * BS;
+      if (need_e) load_energies(k);
       bool ok = mbar_wait(&blk_full[k & 1], (k >> 1) & 1, abort_flag, kSpinLimit);
       // tcgen05.ld/st are warp-collective: the whole warp takes one branch.
       if (!__all_sync(0xffffffffu, ok)) break;
@@ -834,57 +700,59 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&buf_free[k & 1]);
+      // The block's completed slots: window energies (running sums, in
+      // order), scores and stores, specialised per measure.
+      auto slots = [&](auto mt) {
 #pragma unroll
-      for (int g = 0; g < BS; ++g) {
-        const int u = t0 + g;
-        const int yd = a.y0 + u - R + 1;
-        if (u >= nsteps) break;
-        // Every step's energy entry is waited for and released in order, so
-        // the ring's barriers never run two phases apart.
-        ST e[S];
+        for (int g = 0; g < BS; ++g) {
+          const int u = t0 + g;
+          const int yd = ea_y0 + u - R + 1;
+          if (u >= nsteps) break;
+          double e[S];
 #pragma unroll
-        for (int p = 0; p < S; ++p) e[p] = ST(0);
-        if (need_e) {
-          ok = mbar_wait(&e_full[u % kNE], (u / kNE) & 1, abort_flag, kSpinLimit);
-          if (!__all_sync(0xffffffffu, ok)) break;
-          const ST* ep = estage + (u % kNE) * P + S * m;
+          for (int p = 0; p < S; ++p) {
+            esum[p] += static_cast<double>(rin[g][p]) - static_cast<double>(rout[g][p]);
+            e[p] = esum[p];
+          }
+          if (u >= R - 1 && yd < ea_yend) {
+            char* orow = ea_dst + (size_t)yd * ea_dst_pitch;
+            const int x0 = xl;
+            if (ea_nch == 1 && !ea_dst_f64 && x0 + S <= ea_W) {
+              float outf[S];
 #pragma unroll
-          for (int p = 0; p < S; ++p) e[p] = ep[p];
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&e_free[u % kNE]);
-        }
-        if (u >= R - 1 && yd < a.yend) {
-          char* orow = a.dst + (size_t)yd * a.dst_pitch;
-          const int x0 = a.xs_out + S * m;
-          if (a.nch == 1 && !a.dst_f64 && x0 + S <= a.W) {
-            float outf[S];
+              for (int p = 0; p < S; ++p) outf[p] = score_f(mt, val[g * S + p], e[p]);
+              float* o = reinterpret_cast<float*>(orow) + x0;
+              if (S % 4 == 0) {
 #pragma unroll
-            for (int p = 0; p < S; ++p) outf[p] = score_f(val[g * S + p], e[p]);
-            float* o = reinterpret_cast<float*>(orow) + x0;
-            if (S % 4 == 0) {
+                for (int j = 0; j < S / 4; ++j)
+                  reinterpret_cast<float4*>(o)[j] = make_float4(
+                      outf[(4 * j) % S], outf[(4 * j + 1) % S], outf[(4 * j + 2) % S],
+                      outf[(4 * j + 3) % S]);
+              } else {
 #pragma unroll
-              for (int j = 0; j < S / 4; ++j)
-                reinterpret_cast<float4*>(o)[j] = make_float4(
-                    outf[(4 * j) % S], outf[(4 * j + 1) % S], outf[(4 * j + 2) % S],
-                    outf[(4 * j + 3) % S]);
+                for (int j = 0; j < S / 2; ++j)
+                  reinterpret_cast<float2*>(o)[j] = make_float2(outf[(2 * j) % S], outf[(2 * j + 1) % S]);
+              }
             } else {
 #pragma unroll
-              for (int j = 0; j < S / 2; ++j)
-                reinterpret_cast<float2*>(o)[j] = make_float2(outf[(2 * j) % S], outf[(2 * j + 1) % S]);
-            }
-          } else {
-#pragma unroll
-            for (int p = 0; p < S; ++p) {
-              const int x = x0 + p;
-              if (x >= a.W) break;
-              const size_t xo = (size_t)x * a.nch + ch;
-              if (a.dst_f64)
-                reinterpret_cast<double*>(orow)[xo] = score_d(val[g * S + p], e[p]);
-              else
-                reinterpret_cast<float*>(orow)[xo] = score_f(val[g * S + p], e[p]);
+              for (int p = 0; p < S; ++p) {
+                const int x = x0 + p;
+                if (x >= ea_W) break;
+                const size_t xo = (size_t)x * ea_nch + ch;
+                if (ea_dst_f64)
+                  reinterpret_cast<double*>(orow)[xo] = score_d(mt, val[g * S + p], e[p]);
+                else
+                  reinterpret_cast<float*>(orow)[xo] = score_f(mt, val[g * S + p], e[p]);
+              }
             }
           }
         }
+      };
+      switch (ea_measure) {
+        case kSqrDistance: slots(std::integral_constant<int, kSqrDistance>()); break;
+        case kSqrDistanceNorm: slots(std::integral_constant<int, kSqrDistanceNorm>()); break;
+        case kCrossCorrNorm: slots(std::integral_constant<int, kCrossCorrNorm>()); break;
+        default: slots(std::integral_constant<int, kCrossCorr>()); break;
       }
       if (!__all_sync(0xffffffffu, ok)) break;
     }
@@ -898,14 +766,7 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
       mbar_inval(&raw_full[i]);
       mbar_inval(&raw_free[i]);
     }
-    for (int i = 0; i < kNA; ++i) {
-      mbar_inval(&ready[i]);
-      mbar_inval(&mma_done[i]);
-    }
-    for (int i = 0; i < kNE; ++i) {
-      mbar_inval(&e_full[i]);
-      mbar_inval(&e_free[i]);
-    }
+    for (int i = 0; i < G.NA; ++i) mbar_inval(&ready[i]);
     for (int i = 0; i < 2; ++i) {
       mbar_inval(&blk_full[i]);
       mbar_inval(&buf_free[i]);
@@ -949,7 +810,13 @@ struct BatchDest {
 };
 struct BatchItem {
   int img, tpl, dst;  // indices into the tables
+  int energy;         // index into the energy maps, -1 for CrossCorr
   int ch, strip, y0, yend;
+};
+// Window-energy map of one (image, template size) pair of a batch.
+struct BatchEnergy {
+  const char* ptr;
+  size_t pitch, plane;
 };
 
 struct TensorLaunch {
@@ -967,6 +834,7 @@ struct TensorLaunch {
   const BatchTemplate* tpls;
   const BatchDest* dsts;
   const BatchItem* items;
+  const BatchEnergy* energies;
   int nitems;
   int* counter;        // next item; reset to 0 before every launch
 };
@@ -1030,6 +898,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.dst_pitch = ds.pitch;
           item.dst_f64 = ds.f64;
           item.measure = P.measure;
+          item.energy = nullptr;
+          item.e_pitch = item.e_plane = 0;
+          if (bi.energy >= 0) {
+            const BatchEnergy be = P.energies[bi.energy];
+            item.energy = be.ptr;
+            item.e_pitch = be.pitch;
+            item.e_plane = be.plane;
+          }
         }
       }
       __syncthreads();
@@ -1214,6 +1090,18 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
   const int smem_bytes = smem_for<ELEM>(cls, tmpl.width, ax, P.nbox);
   if (smem_bytes > kMaxDynSmem) return cudaErrorInvalidValue;
 
+  // Row energies of every source row, for the measures that use them.
+  if (m != kCrossCorr) {
+    const size_t ep = row_energy_pitch(src.width);
+    const size_t eplane = ep * src.height;
+    char* emap = reinterpret_cast<char*>(ctx.scratch(Context::kEnergyMap, eplane * src.nch));
+    cudaError_t ee = launch_row_energy(src, tmpl.width, ax, emap, ep, eplane, ctx.stream);
+    if (ee != cudaSuccess) return ee;
+    a.energy = emap;
+    a.e_pitch = ep;
+    a.e_plane = eplane;
+  }
+
   // Source planes: the image itself for one channel, else a split copy.
   const void* planes = src.ptr;
   size_t plane_pitch = src.pitch;
@@ -1259,17 +1147,33 @@ struct TensorBatch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::map<int, int> bh;  // class -> band height used
+  // Row-energy maps, one per (image, template width) of the batch (measures
+  // other than CrossCorr), recomputed by every run.
+  struct EnergyJob {
+    int img, tw;
+    size_t offset, pitch, plane;
+  };
+  std::vector<EnergyJob> ejobs;
+  char* emaps = nullptr;
 };
 
 namespace {
 
-// Channel splits, queue reset, persistent launch. `count` is false while the
-// work is recorded into a graph (counted when the graph is launched).
+// Channel splits, window energies, queue reset, persistent launch. `count`
+// is false while the work is recorded into a graph (counted when the graph
+// is launched).
 template <int ELEM>
 cudaError_t batch_record(TensorBatch& b, cudaStream_t stream, bool count) {
   for (size_t i = 0; i < b.images.size(); ++i) {
     if (b.plane_offsets[i].first)
       split_channels<ELEM>(b.images[i], b.planes + b.plane_offsets[i].second, stream, count);
+  }
+  for (const TensorBatch::EnergyJob& j : b.ejobs) {
+    const unsigned long long before = g_launches;
+    cudaError_t ee = launch_row_energy(b.images[j.img], j.tw, j.tw / 2, b.emaps + j.offset,
+                                       j.pitch, j.plane, stream);
+    if (ee != cudaSuccess) return ee;
+    if (!count) g_launches = before;
   }
   cudaError_t e = cudaMemsetAsync(b.launch.counter, 0, sizeof(int), stream);
   if (e != cudaSuccess) return e;
@@ -1287,6 +1191,7 @@ std::vector<BatchItem> make_items(const std::vector<DevImage>& imgs,
                                   const std::vector<int>& pair_img,
                                   const std::vector<int>& pair_tpl,
                                   const std::vector<int>& pair_dst,
+                                  const std::vector<int>& pair_energy,
                                   const std::map<int, int>& bh) {
   std::vector<std::pair<long long, BatchItem>> v;
   for (size_t p = 0; p < pair_img.size(); ++p) {
@@ -1305,6 +1210,7 @@ std::vector<BatchItem> make_items(const std::vector<DevImage>& imgs,
           it.img = pair_img[p];
           it.tpl = pair_tpl[p];
           it.dst = pair_dst[p];
+          it.energy = pair_energy[p];
           it.ch = c;
           it.strip = st;
           it.y0 = y0;
@@ -1330,14 +1236,16 @@ cudaError_t upload_tables(TensorBatch& b, const std::vector<CUtensorMap>& maps,
                           const std::vector<BatchImage>& bimgs,
                           const std::vector<BatchTemplate>& btpls,
                           const std::vector<BatchDest>& bdsts,
-                          const std::vector<BatchItem>& items, void** mem) {
+                          const std::vector<BatchItem>& items,
+                          const std::vector<BatchEnergy>& benergy, void** mem) {
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t o_maps = 0;
   const size_t o_imgs = al(o_maps + maps.size() * sizeof(CUtensorMap));
   const size_t o_tpls = al(o_imgs + bimgs.size() * sizeof(BatchImage));
   const size_t o_dsts = al(o_tpls + btpls.size() * sizeof(BatchTemplate));
   const size_t o_items = al(o_dsts + bdsts.size() * sizeof(BatchDest));
-  const size_t o_ctr = al(o_items + items.size() * sizeof(BatchItem));
+  const size_t o_en = al(o_items + items.size() * sizeof(BatchItem));
+  const size_t o_ctr = al(o_en + benergy.size() * sizeof(BatchEnergy));
   const size_t total = o_ctr + 256;
   std::vector<char> host(total, 0);
   std::memcpy(host.data() + o_maps, maps.data(), maps.size() * sizeof(CUtensorMap));
@@ -1345,6 +1253,8 @@ cudaError_t upload_tables(TensorBatch& b, const std::vector<CUtensorMap>& maps,
   std::memcpy(host.data() + o_tpls, btpls.data(), btpls.size() * sizeof(BatchTemplate));
   std::memcpy(host.data() + o_dsts, bdsts.data(), bdsts.size() * sizeof(BatchDest));
   std::memcpy(host.data() + o_items, items.data(), items.size() * sizeof(BatchItem));
+  if (!benergy.empty())
+    std::memcpy(host.data() + o_en, benergy.data(), benergy.size() * sizeof(BatchEnergy));
   char* d = nullptr;
   cudaError_t e = cudaMalloc(&d, total);
   if (e != cudaSuccess) return e;
@@ -1360,6 +1270,7 @@ cudaError_t upload_tables(TensorBatch& b, const std::vector<CUtensorMap>& maps,
   P.tpls = reinterpret_cast<const BatchTemplate*>(d + o_tpls);
   P.dsts = reinterpret_cast<const BatchDest*>(d + o_dsts);
   P.items = reinterpret_cast<const BatchItem*>(d + o_items);
+  P.energies = reinterpret_cast<const BatchEnergy*>(d + o_en);
   P.nitems = static_cast<int>(items.size());
   P.counter = reinterpret_cast<int*>(d + o_ctr);
   return cudaSuccess;
@@ -1393,15 +1304,28 @@ int autotune_bh(Context& ctx, int measure, const DevImage& img, const CUtensorMa
   std::vector<BatchTemplate> btpls(1, BatchTemplate{(const char*)tpl.ptr, tpl.pitch, tpl.width,
                                                     tpl.height, cls});
   std::vector<BatchDest> bdsts(1, BatchDest{probe_dst, probe_pitch, 0});
+  // The probe pair's row energies, computed once for every candidate.
+  std::vector<BatchEnergy> benergy;
+  char* probe_e = nullptr;
+  if (measure != kCrossCorr) {
+    const size_t ep = row_energy_pitch(img.width), eplane = ep * img.height;
+    if (cudaMalloc(&probe_e, eplane * img.nch) != cudaSuccess) return cand.back();
+    if (launch_row_energy(img, tpl.width, tpl.width / 2, probe_e, ep, eplane, ctx.stream) !=
+        cudaSuccess) {
+      cudaFree(probe_e);
+      return cand.back();
+    }
+    benergy.push_back(BatchEnergy{probe_e, ep, eplane});
+  }
   float best = 1e30f;
   int best_bh = cand.back();
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   for (int bh : cand) {
-    std::vector<int> pi(reps, 0), pt(reps, 0), pd(reps, 0);
+    std::vector<int> pi(reps, 0), pt(reps, 0), pd(reps, 0), pe(reps, probe_e ? 0 : -1);
     std::map<int, int> m1{{cls, bh}};
-    std::vector<BatchItem> items = make_items<ELEM>({img}, {tpl}, pi, pt, pd, m1);
+    std::vector<BatchItem> items = make_items<ELEM>({img}, {tpl}, pi, pt, pd, pe, m1);
     TensorBatch tb;
     tb.ctx = &ctx;
     std::memset(&tb.launch, 0, sizeof(tb.launch));
@@ -1411,7 +1335,8 @@ int autotune_bh(Context& ctx, int measure, const DevImage& img, const CUtensorMa
     tb.launch.err = reinterpret_cast<int*>(ctx.scratch(Context::kTensorAux, 256));
     tb.smem = smem;
     void* mem = nullptr;
-    if (upload_tables<ELEM>(tb, maps, bimgs, btpls, bdsts, items, &mem) != cudaSuccess) break;
+    if (upload_tables<ELEM>(tb, maps, bimgs, btpls, bdsts, items, benergy, &mem) != cudaSuccess)
+      break;
     float ms = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
       cudaEventRecord(e0, ctx.stream);
@@ -1430,6 +1355,10 @@ int autotune_bh(Context& ctx, int measure, const DevImage& img, const CUtensorMa
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (probe_e) {
+    cudaStreamSynchronize(ctx.stream);
+    cudaFree(probe_e);
+  }
   return best_bh;
 }
 
@@ -1535,19 +1464,41 @@ TensorBatch* batch_create(Context& ctx, Measure m, const std::vector<DevImage>& 
   }
   b->bh = bh;
 
-  std::vector<int> pi, pt, pd;
+  // Row-energy maps: one per (image, template width) for the measures that
+  // use them, laid out back to back in one allocation owned by the batch.
+  std::map<std::pair<int, int>, int> eidx;
+  std::vector<BatchEnergy> benergy;
+  if (m != kCrossCorr) {
+    size_t total = 0;
+    for (size_t i = 0; i < imgs.size(); ++i)
+      for (const DevImage& t : tpls) {
+        const auto key = std::make_pair((int)i, t.width);
+        if (eidx.count(key)) continue;
+        eidx[key] = (int)b->ejobs.size();
+        const size_t ep = row_energy_pitch(imgs[i].width);
+        const size_t eplane = ep * imgs[i].height;
+        b->ejobs.push_back(TensorBatch::EnergyJob{(int)i, t.width, total, ep, eplane});
+        total += eplane * imgs[i].nch;
+      }
+    e = cudaMalloc(&b->emaps, total);
+    if (e != cudaSuccess) return fail(e);
+    for (const TensorBatch::EnergyJob& j : b->ejobs)
+      benergy.push_back(BatchEnergy{b->emaps + j.offset, j.pitch, j.plane});
+  }
+  std::vector<int> pi, pt, pd, pe;
   for (size_t i = 0; i < imgs.size(); ++i)
     for (size_t j = 0; j < tpls.size(); ++j) {
       pi.push_back((int)i);
       pt.push_back((int)j);
       pd.push_back((int)(i * tpls.size() + j));
+      pe.push_back(m != kCrossCorr ? eidx[std::make_pair((int)i, tpls[j].width)] : -1);
     }
-  std::vector<BatchItem> items = make_items<ELEM>(imgs, tpls, pi, pt, pd, bh);
+  std::vector<BatchItem> items = make_items<ELEM>(imgs, tpls, pi, pt, pd, pe, bh);
   b->launch.mode = 1;
   b->launch.measure = m;
   b->launch.nbox = b->nbox;
   b->launch.err = reinterpret_cast<int*>(ctx.scratch(Context::kTensorAux, 256));
-  e = upload_tables<ELEM>(*b, maps, bimgs, btpls, bdsts, items, &b->tables);
+  e = upload_tables<ELEM>(*b, maps, bimgs, btpls, bdsts, items, benergy, &b->tables);
   if (e != cudaSuccess) return fail(e);
   b->nitems = b->launch.nitems;
   b->smem = 0;
@@ -1634,8 +1585,9 @@ TensorBatch* tensor_batch_create(Context& ctx, Measure m, const std::vector<DevI
 }
 
 cudaError_t tensor_batch_run(TensorBatch* b) {
-  count_launches(1 + std::count_if(b->plane_offsets.begin(), b->plane_offsets.end(),
-                                   [](const std::pair<int, size_t>& p) { return p.first != 0; }));
+  count_launches(1 + (int)b->ejobs.size() +
+                 std::count_if(b->plane_offsets.begin(), b->plane_offsets.end(),
+                               [](const std::pair<int, size_t>& p) { return p.first != 0; }));
   return cudaGraphLaunch(b->exec, b->ctx->stream);
 }
 
@@ -1654,6 +1606,7 @@ void tensor_batch_destroy(TensorBatch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->tables) cudaFree(b->tables);
   if (b->planes) cudaFree(b->planes);
+  if (b->emaps) cudaFree(b->emaps);
   delete b;
 }
 
