@@ -198,8 +198,9 @@ ocipError ocip_API ocipCrossCorr_Norm(ocipImage Source, ocipImage Template,
 
 /* ---- Proximity entry points named after the FFT path ------------------- */
 /* (reference include/OpenCLIPP.h:673-688). The reference computes these with
- * clFFT on F32, 1-channel images. Here they compute the same measures on the
- * tensor-core path (no FFT); ocipIsFFTAvailable() returns 1. */
+ * clFFT on F32, 1-channel images, for large templates. Here they compute the
+ * same measures on the tensor-core path (no FFT), templates beyond 64 x 64 as
+ * tiles whose product sums add up in FP64; ocipIsFFTAvailable() returns 1. */
 ocipBool ocip_API ocipIsFFTAvailable(void);
 ocipError ocip_API ocipPrepareImageProximityFFT(ocipProgram* ProgramPtr,
                                                 ocipImage Image,

@@ -18,9 +18,11 @@ extern "C" {
  *   OCIP_PATH_TENSOR: tcgen05 tensor cores for the product term of
  *                     SqrDistance[_Norm] and CrossCorr[_Norm] (i8 MMA with exact
  *                     s32 sums for U8 sources, split BF16 for F32 and U16;
- *                     1-4 channels; templates up to 64 x 64) with FP64/int32
- *                     window statistics; AbsDistance and shapes the tensor
- *                     kernels do not cover fall back to PLAIN.
+ *                     1-4 channels; templates up to 1024 columns: beyond
+ *                     64 x 64 they run as tiles of at most 64 x 64 whose
+ *                     product sums add up in FP64) with FP64/exact window
+ *                     statistics; AbsDistance and shapes the tensor kernels
+ *                     do not cover fall back to PLAIN.
  *   OCIP_PATH_AUTO  : TENSOR where it is exact (8-bit sources), PLAIN
  *                     otherwise. */
 enum ocipProximityPath {

@@ -31,8 +31,10 @@ struct Context {
     kPlanes = 1,
     kTensorAux = 2,
     kBackward = 3,
-    kEnergyMap = 4,  // window energies of the tensor path (FP64 planes)
-    kNumScratch = 5
+    kEnergyMap = 4,      // row energies of the tensor path
+    kProductMap = 5,     // F64 product sums of templates tiled over launches
+    kTemplateStats = 6,  // per-channel template energy (FP64)
+    kNumScratch = 7
   };
   int device = 0;
   int sm_count = 0;

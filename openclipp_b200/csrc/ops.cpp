@@ -231,7 +231,10 @@ void batch_prepare(ocipProgram* out, int measure, const ocipImage* himgs, int ni
         fail(CL_INVALID_VALUE, "Different number of channels used");
       if (!type_is_float((int)D.desc.Type))
         fail(CL_INVALID_VALUE, "non-float image used when not allowed");
-      if (!tensor_supports((Measure)measure, dev_view(S), dev_view(T), dev_view(D), true))
+      // The persistent batch kernel takes one template per work item: 64 x 64
+      // at most (larger templates are tiled over launches by the one-pair calls).
+      if (!tensor_supports((Measure)measure, dev_view(S), dev_view(T), dev_view(D), true) ||
+          T.desc.Width > 64 || T.desc.Height > 64)
         fail(CL_INVALID_VALUE,
              "batches run on the tensor path: U8, U16 or F32 sources, templates of 64 x 64 "
              "or less (F32 and U16: at least 64 pixels)");

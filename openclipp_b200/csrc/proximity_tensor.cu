@@ -193,6 +193,9 @@ struct ItemArgs {
   // of R(x, r), plane ch at energy + ch * e_plane bytes, rows e_pitch apart.
   const char* energy;
   size_t e_pitch, e_plane;
+  // 1: add the scores (raw CrossCorr sums into an F64 map) to the
+  // destination instead of writing them (templates tiled over launches).
+  int accum;
 };
 
 // Shared-memory layout, identical on host and device.
@@ -545,6 +548,7 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     // The item's fields in registers: the item lives in shared memory, and
     // the score loop would otherwise reload them on every slot.
     const auto ea_W = a.W;
+    const auto ea_accum = a.accum;
     const auto ea_dst = a.dst;
     const auto ea_dst_f64 = a.dst_f64;
     const auto ea_dst_pitch = a.dst_pitch;
@@ -739,7 +743,9 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
                 const int x = x0 + p;
                 if (x >= ea_W) break;
                 const size_t xo = (size_t)x * ea_nch + ch;
-                if (ea_dst_f64)
+                if (ea_dst_f64 && ea_accum)
+                  reinterpret_cast<double*>(orow)[xo] += score_d(mt, val[g * S + p], e[p]);
+                else if (ea_dst_f64)
                   reinterpret_cast<double*>(orow)[xo] = score_d(mt, val[g * S + p], e[p]);
                 else
                   reinterpret_cast<float*>(orow)[xo] = score_f(mt, val[g * S + p], e[p]);
@@ -898,6 +904,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.dst_pitch = ds.pitch;
           item.dst_f64 = ds.f64;
           item.measure = P.measure;
+          item.accum = 0;
           item.energy = nullptr;
           item.e_pitch = item.e_plane = 0;
           if (bi.energy >= 0) {
@@ -1056,7 +1063,7 @@ size_t plane_set_bytes(const DevImage& s) {
 
 template <int ELEM>
 cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevImage& tmpl,
-                       const DevImage& dst, int ax, int ay) {
+                       const DevImage& dst, int ax, int ay, bool accum = false) {
   const int cls = class_of(tmpl.height);
   const int R = class_r(cls);
   TensorLaunch P;
@@ -1086,6 +1093,7 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
   a.dst_pitch = dst.pitch;
   a.dst_f64 = dst.type == F64;
   a.measure = m;
+  a.accum = accum ? 1 : 0;
 
   const int smem_bytes = smem_for<ELEM>(cls, tmpl.width, ax, P.nbox);
   if (smem_bytes > kMaxDynSmem) return cudaErrorInvalidValue;
@@ -1552,7 +1560,9 @@ bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl, const
                      bool forced) {
   if (m == kAbsDistance) return false;
   if (src.nch != tmpl.nch || src.nch != dst.nch || src.nch < 1 || src.nch > 4) return false;
-  if (tmpl.width > 64 || tmpl.height > 64) return false;
+  // Templates beyond 64 x 64 run as tiles of at most 64 x 64 (tensor_large.cu);
+  // the row energies take templates up to 1024 columns.
+  if (tmpl.width > 1024) return false;
   if (src.type == U8) return true;
   // F32 and U16 use the BF16 hi + lo split: about 16 bits of each F32 operand
   // (all 16 of a U16), so one product can be off by ~3e-5 relative; the 1e-5
@@ -1564,6 +1574,7 @@ bool tensor_supports(Measure m, const DevImage& src, const DevImage& tmpl, const
 
 cudaError_t launch_proximity_tensor(Context& ctx, Measure m, const DevImage& src,
                                     const DevImage& tmpl, const DevImage& dst) {
+  if (tmpl.width > 64 || tmpl.height > 64) return launch_proximity_tensor_large(ctx, m, src, tmpl, dst);
   return launch_proximity_tensor_anchored(ctx, m, src, tmpl, dst, tmpl.width / 2,
                                           tmpl.height / 2);
 }
@@ -1574,6 +1585,15 @@ cudaError_t launch_proximity_tensor_anchored(Context& ctx, Measure m, const DevI
   if (src.type == U8) return launch_one<kU8>(ctx, m, src, tmpl, dst, ax, ay);
   if (src.type == U16) return launch_one<kU16>(ctx, m, src, tmpl, dst, ax, ay);
   return launch_one<kF32>(ctx, m, src, tmpl, dst, ax, ay);
+}
+
+cudaError_t launch_tensor_product_sums(Context& ctx, const DevImage& src, const DevImage& tmpl,
+                                       const DevImage& c_map, int ax, int ay, bool accumulate) {
+  if (c_map.type != F64) return cudaErrorInvalidValue;
+  if (src.type == U8) return launch_one<kU8>(ctx, kCrossCorr, src, tmpl, c_map, ax, ay, accumulate);
+  if (src.type == U16)
+    return launch_one<kU16>(ctx, kCrossCorr, src, tmpl, c_map, ax, ay, accumulate);
+  return launch_one<kF32>(ctx, kCrossCorr, src, tmpl, c_map, ax, ay, accumulate);
 }
 
 TensorBatch* tensor_batch_create(Context& ctx, Measure m, const std::vector<DevImage>& imgs,

@@ -24,6 +24,21 @@ cudaError_t launch_proximity_tensor_anchored(Context& ctx, Measure m, const DevI
                                              const DevImage& tmpl, const DevImage& dst, int ax,
                                              int ay);
 
+// Product sums C(x, y) = sum_{w, h} S(x + w - ax, y + h - ay) T(w, h) of one
+// template of at most 64 x 64 (a tile of a larger one) on the tensor cores,
+// written into (accumulate = false) or added to (true) the F64 map c_map of
+// the source's size and channels. Any anchor, including ones outside the
+// template (a tile's offset within the whole template).
+cudaError_t launch_tensor_product_sums(Context& ctx, const DevImage& src, const DevImage& tmpl,
+                                       const DevImage& c_map, int ax, int ay, bool accumulate);
+
+// A measure of a template larger than 64 x 64 (up to 1024 columns): the
+// template is cut into tiles of at most 64 x 64 whose product sums accumulate
+// in an F64 map, and a scoring pass adds the window energies (row energies
+// plus running column sums) and the template energy.
+cudaError_t launch_proximity_tensor_large(Context& ctx, Measure m, const DevImage& src,
+                                          const DevImage& tmpl, const DevImage& dst);
+
 // Gradients of L = sum G1 * SqrDistance(S, T) + sum G2 * CrossCorr_Norm(S, T)
 // (F32 sources, one channel, templates up to 64 x 64) into dS (S's size) and
 // dT (T's size), F32 or F64; G1 or G2 may be null, N2 is CrossCorr_Norm(S, T)

@@ -133,9 +133,9 @@ def test_f32_signed_values(ocip, ctx):
 
 
 def test_fallbacks_to_plain(ocip, ctx):
-    """AbsDistance, types without a tensor form, small F32 templates and large
-    templates are served by the plain path even when the tensor path is
-    requested."""
+    """AbsDistance, types without a tensor form, small F32 templates and
+    templates wider than 1024 columns are served by the plain path even when
+    the tensor path is requested."""
     ctx.make_current()
     rng = np.random.default_rng(5)
     S = rng.random((80, 90)).astype(np.float32)
@@ -154,8 +154,9 @@ def test_fallbacks_to_plain(ocip, ctx):
     _, path = run(ocip, ctx, 3, S16, rng.integers(0, 65535, (9, 9), dtype=np.uint16),
                   ocip.PATH_AUTO)
     assert path == ocip.PATH_PLAIN
-    _, path = run(ocip, ctx, 3, rng.random((100, 100)).astype(np.float32),
-                  rng.random((65, 65)).astype(np.float32), ocip.PATH_TENSOR)
+    # templates wider than the row-energy pass takes (1024 columns)
+    _, path = run(ocip, ctx, 3, rng.random((12, 1100)).astype(np.float32),
+                  rng.random((2, 1030)).astype(np.float32), ocip.PATH_TENSOR)
     assert path == ocip.PATH_PLAIN
     # AUTO keeps F32 on the plain path (not bit-exact on the tensor path)
     _, path = run(ocip, ctx, 3, S, T, ocip.PATH_AUTO)
