@@ -57,10 +57,31 @@ Image& image(ocipImage h) {
   return *img;
 }
 
+// Counts a transfer of the image's host buffer and page-locks a pageable
+// buffer once it has been transferred Image::kRegisterAfter times. A buffer
+// that cannot be registered (already registered as part of another range,
+// or the pinned-memory limit reached) stays pageable; copies are correct
+// either way.
+void note_host_transfer(Image& img) {
+  if (img.host_pinned || img.host_transfers < 0) return;
+  if (++img.host_transfers < Image::kRegisterAfter) return;
+  // The caller's rows: Step bytes apart, the last one row_bytes() long.
+  const size_t bytes = (size_t)img.desc.Step * (img.desc.Height - 1) + img.row_bytes();
+  const cudaError_t e = cudaHostRegister(img.host, bytes, cudaHostRegisterDefault);
+  if (e == cudaSuccess) {
+    img.host_pinned = img.host_registered = true;
+  } else {
+    cudaGetLastError();  // not sticky: clear it
+    if (e == cudaErrorHostMemoryAlreadyRegistered) img.host_pinned = true;
+    else img.host_transfers = -1;  // do not try again
+  }
+}
+
 void send(Image& img) {
   if (img.host == nullptr) return;  // device-only image (Buffer.cpp:158)
   Context& ctx = *img.ctx;
   check_cuda(cudaSetDevice(ctx.device), "cudaSetDevice");
+  note_host_transfer(img);
   const size_t row = img.row_bytes();
   check_cuda(cudaMemcpy2DAsync(img.dev, img.pitch, img.host, img.desc.Step, row,
                                img.desc.Height, cudaMemcpyHostToDevice, ctx.stream),
@@ -247,6 +268,13 @@ ocipError ocipCreateImage(ocipImage* ImagePtr, SImage desc, void* ImageData,
     img->ctx = &ctx;
     img->desc = desc;
     img->host = ImageData;
+    if (ImageData != nullptr) {
+      cudaPointerAttributes attr;
+      if (cudaPointerGetAttributes(&attr, ImageData) == cudaSuccess)
+        img->host_pinned = attr.type == cudaMemoryTypeHost;
+      else
+        cudaGetLastError();
+    }
     img->pitch = (row + 127) / 128 * 128;
     cudaError_t e = cudaMalloc(&img->dev, img->pitch * desc.Height);
     if (e != cudaSuccess) {
@@ -284,6 +312,7 @@ ocipError ocipReadImage(ocipImage h) {
     // this map travels to the host. The call still returns only once the
     // data is in the host buffer (Read is blocking, OpenCLIPP.cpp:203-211),
     // so no copy is ever left in flight across calls.
+    note_host_transfer(img);
     if (img.exposed) mark_written(img);  // writes through the raw address: wait for all
     if (img.written) check_cuda(cudaStreamWaitEvent(ctx.copy_stream, img.written, 0), "read wait");
     if (ctx.untracked)
@@ -305,6 +334,7 @@ ocipError ocipReleaseImage(ocipImage h) {
       cudaStreamSynchronize(img->ctx->stream);
     }
     if (img->written) cudaEventDestroy(img->written);
+    if (img->host_registered) cudaHostUnregister(img->host);
     cudaFree(img->dev);
     img->magic = 0;
     delete img;
