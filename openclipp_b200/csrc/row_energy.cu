@@ -11,10 +11,10 @@
 // the rows. Rows are independent here, so every warp streams its own row
 // segment with all its loads in flight.
 //
-// R is stored as FP32 for F32 and U16 sources (an FP64 sum rounded once:
-// relative error 2^-24; an FP64 running sum of FP32 values adds and later
-// removes each value exactly) and as int32 for U8 sources (exact: at most
-// 1024 * 255^2 < 2^31). Bound: HBM (the source read once, 4 bytes written per
+// R is stored as FP32 for F32 and U16 sources (a difference of FP64 prefix
+// sums rounded once: relative error 2^-24; an FP64 running sum of FP32
+// values adds and later removes each value exactly) and as int32 for U8
+// sources (exact). Bound: HBM (the source read once, 4 bytes written per
 // output column and source row).
 #include <cuda_runtime.h>
 
@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kWarps = 8;        // one row segment per warp
 constexpr int kSeg = 256;        // output columns per segment (8 per lane)
-constexpr int kMaxTw = 1024;
+constexpr int kMaxTw = 1024;  // 256 + tw - 1 <= 32 * 41
 
 struct RowEnergyParams {
   const char* src;
@@ -39,22 +39,26 @@ struct RowEnergyParams {
   size_t dst_plane;   // bytes between channel planes
   int W, H, nch;
   int tw, ax;
-  int buf;            // shared-memory entries per warp
 };
 
 template <typename ET>
 struct RowSumOf {
-  // Exact accumulation: int64 for integers, FP64 for floats.
-  typedef typename std::conditional<std::is_integral<ET>::value, long long, double>::type A;
+  // Prefix sums, exact for integers: int32 for 8-bit sources (at most
+  // 1279 * 255^2 < 2^31), FP64 otherwise (16-bit: below 2^53; F32: squares
+  // exact, sums rounded in FP64).
+  typedef typename std::conditional<sizeof(ET) == 1, int, double>::type A;
   // Stored: int32 for 8-bit sources, FP32 otherwise.
   typedef typename std::conditional<sizeof(ET) == 1, int, float>::type R;
 };
 
-// Shared-memory slot of element i of a warp's buffer: one pad slot after
-// every 8, so that lanes reading runs 8 apart fall in different banks.
-__device__ __forceinline__ int rpad(int i) { return i + (i >> 3); }
-
-template <typename ET>
+// One warp per (source row, 256 output columns). The squares of the n =
+// 256 + tw - 1 source pixels the segment's windows cover are staged in
+// shared memory (coalesced loads); lane l turns its K contiguous entries
+// into prefix sums (local prefix plus a warp scan of the lanes' totals),
+// P(i) = sum of squares [0, i) stored at entry i - 1; output column x0 + j
+// (j = lane + 32 u) is then P(j + tw) - P(j): two conflict-free reads, and
+// the warp's stores are 128-byte rows.
+template <typename ET, int K>
 __global__ void __launch_bounds__(kWarps * 32) row_energy_kernel(const RowEnergyParams p) {
   typedef typename RowSumOf<ET>::A A;
   typedef typename RowSumOf<ET>::R RT;
@@ -64,57 +68,59 @@ __global__ void __launch_bounds__(kWarps * 32) row_energy_kernel(const RowEnergy
   if (r >= p.H) return;  // whole warp
   const int c = blockIdx.z;
   const int x0 = blockIdx.x * kSeg;
-  A* buf = reinterpret_cast<A*>(smem) + warp * p.buf;
-  // Squares of source columns x0 - ax .. x0 - ax + kSeg + tw - 2, coalesced.
-  const ET* row = reinterpret_cast<const ET*>(p.src + (size_t)r * p.src_pitch);
+  A* buf = reinterpret_cast<A*>(smem) + warp * (32 * K);
+  const ET* row = reinterpret_cast<const ET*>(p.src + (size_t)r * p.src_pitch) + c;
   const int n = kSeg + p.tw - 1;
   const int xs0 = x0 - p.ax;
-  constexpr int U = 4;  // loads issued before any is used
-  for (int i0 = 0; i0 < n; i0 += 32 * U) {
-    ET v[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * 32 + lane;
-      const int x = xs0 + i;
-      v[u] = (i < n && x >= 0 && x < p.W) ? row[(size_t)x * p.nch + c] : ET(0);
+  // Squares of source columns xs0 .. xs0 + n - 1 (zero outside the image).
+#pragma unroll 4
+  for (int i = lane; i < 32 * K; i += 32) {
+    const int x = xs0 + i;
+    A v = A(0);
+    if (i < n && x >= 0 && x < p.W) {
+      const A e = static_cast<A>(row[x * p.nch]);
+      v = e * e;
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * 32 + lane;
-      if (i < n) {
-        const A a = static_cast<A>(v[u]);
-        buf[rpad(i)] = a * a;
-      }
-    }
+    buf[i] = v;
   }
   __syncwarp();
-  const int xl = x0 + 8 * lane;
-  if (xl >= p.W) return;
-  A e = A(0);
-  for (int w = 0; w < p.tw; ++w) e += buf[rpad(8 * lane + w)];
-  RT o[8];
-  o[0] = static_cast<RT>(e);
+  // Lane l: entries K l .. K l + K - 1 -> inclusive prefix sums in place.
+  A loc[K];
+  A tot = A(0);
 #pragma unroll
-  for (int i = 1; i < 8; ++i) {
-    e += buf[rpad(8 * lane + i - 1 + p.tw)] - buf[rpad(8 * lane + i - 1)];
-    o[i] = static_cast<RT>(e);
+  for (int k = 0; k < K; ++k) {
+    tot += buf[K * lane + k];
+    loc[k] = tot;
   }
-  RT* dst = reinterpret_cast<RT*>(p.dst + c * p.dst_plane + (size_t)r * p.dst_pitch) + xl;
-  if (xl + 8 <= p.W) {
-    reinterpret_cast<uint4*>(dst)[0] = *reinterpret_cast<const uint4*>(&o[0]);
-    reinterpret_cast<uint4*>(dst)[1] = *reinterpret_cast<const uint4*>(&o[4]);
-  } else {
-    for (int i = 0; i < 8 && xl + i < p.W; ++i) dst[i] = o[i];
+  A incl = tot;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const A o = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += o;
+  }
+  const A excl = incl - tot;
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < K; ++k) buf[K * lane + k] = excl + loc[k];
+  __syncwarp();
+  RT* dst = reinterpret_cast<RT*>(p.dst + c * p.dst_plane + (size_t)r * p.dst_pitch);
+#pragma unroll
+  for (int u = 0; u < kSeg / 32; ++u) {
+    const int j = lane + 32 * u;
+    const int x = x0 + j;
+    if (x < p.W) {
+      const A hi = buf[j + p.tw - 1];
+      const A lo = j > 0 ? buf[j - 1] : A(0);
+      dst[x] = static_cast<RT>(hi - lo);
+    }
   }
 }
 
-template <typename ET>
-cudaError_t launch_typed(RowEnergyParams p, cudaStream_t st) {
+template <typename ET, int K>
+cudaError_t launch_k(const RowEnergyParams& p, cudaStream_t st) {
   typedef typename RowSumOf<ET>::A A;
-  const int n = kSeg + p.tw - 1;
-  p.buf = n + (n >> 3) + 1;
-  const size_t smem = (size_t)kWarps * p.buf * sizeof(A);
-  auto kern = row_energy_kernel<ET>;
+  const size_t smem = (size_t)kWarps * 32 * K * sizeof(A);
+  auto kern = row_energy_kernel<ET, K>;
   if (smem > 48 * 1024) {
     const cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -124,6 +130,16 @@ cudaError_t launch_typed(RowEnergyParams p, cudaStream_t st) {
   kern<<<grid, kWarps * 32, smem, st>>>(p);
   count_launches(1);
   return cudaGetLastError();
+}
+
+template <typename ET>
+cudaError_t launch_typed(const RowEnergyParams& p, cudaStream_t st) {
+  // K: staged entries per lane, 32 K >= 256 + tw - 1.
+  const int n = kSeg + p.tw - 1;
+  if (n <= 32 * 9) return launch_k<ET, 9>(p, st);
+  if (n <= 32 * 11) return launch_k<ET, 11>(p, st);
+  if (n <= 32 * 17) return launch_k<ET, 17>(p, st);
+  return launch_k<ET, 41>(p, st);
 }
 
 }  // namespace
@@ -144,7 +160,6 @@ cudaError_t launch_row_energy(const DevImage& src, int tw, int ax, void* dst, si
   p.nch = src.nch;
   p.tw = tw;
   p.ax = ax;
-  p.buf = 0;
   switch (src.type) {
     case U8: return launch_typed<uint8_t>(p, stream);
     case U16: return launch_typed<uint16_t>(p, stream);
