@@ -372,6 +372,12 @@ def run_ours(args, world, rank, local):
         acc.update(accuracy_suite(ocip, ctx, S, (ty, tx), product))
         ctx.set_path(path)
 
+    # Best match of the step's CrossCorr_Norm map: ocipMaxIndx on a written map
+    # against the reduction fused into the scoring epilogue (no map written).
+    best = best_match_timing(ocip, torch, ctx, stream, flush, Si, Ti, Ds[MEASURES.index(
+        "CrossCorr_Norm")]) if ("CrossCorr_Norm" in MEASURES and not args.no_plain_arm) else None
+    ctx.set_path(path)
+
     # End-to-end arm: pinned host buffers, send + calls + reads per step.
     e2e_ms = run_e2e(args, ocip, torch, ctx, S, T, stream) if not args.no_e2e else float("nan")
     e2e_ms = allreduce_max(e2e_ms)
@@ -428,6 +434,7 @@ def run_ours(args, world, rank, local):
         "tensor_over_plain": {m: round(med_plain[m] / med[m], 2) for m in med_plain
                               if paths_used.get(m) == "tensor"},
         "accuracy_vs_fp64": acc,
+        "best_match": best,
         "roofline": roof,
         "roofline_plain": roof_plain,
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Gtaps/s",
@@ -453,6 +460,47 @@ def run_ours(args, world, rank, local):
 
 
 MEAS_ALL = ["SqrDistance", "SqrDistance_Norm", "AbsDistance", "CrossCorr", "CrossCorr_Norm"]
+
+
+def best_match_timing(ocip, torch, ctx, stream, flush, Si, Ti, Di, reps=10):
+    """CUDA-event ms of the best match of CrossCorr_Norm (MaxIndx), tensor
+    path: the map written then ocipMaxIndx, against ocipProximityIndx with
+    the reduction in the scoring epilogue and no map. L2 flushed before each."""
+    ctx.set_path(ocip.PATH_TENSOR)
+    prog = ocip.prepare_statistics(Di)
+
+    def map_then_index():
+        ocip.check(ocip.proximity("CrossCorr_Norm", Si, Ti, Di), "CrossCorr_Norm")
+        rc, v, x, y = ocip.index_reduce("MaxIndx", prog, Di)
+        ocip.check(rc, "ocipMaxIndx")
+        return v, x, y
+
+    def fused():
+        rc, v, x, y = ocip.proximity_index("CrossCorr_Norm", "MaxIndx", Si, Ti)
+        ocip.check(rc, "ocipProximityIndx")
+        return v, x, y
+
+    out = {}
+    answers = {}
+    for name, fn in (("map_then_index_ms", map_then_index), ("fused_no_map_ms", fused)):
+        for _ in range(3):
+            answers[name] = fn()
+        t = []
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+        out[name] = round(float(np.median(t)), 4)
+    prog.release()
+    out["same_answer"] = answers["map_then_index_ms"] == answers["fused_no_map_ms"]
+    out["answer"] = list(answers["fused_no_map_ms"])
+    out["measure"], out["reduction"] = "CrossCorr_Norm", "MaxIndx"
+    return out
 
 
 def _run_maps(ocip, ctx, path, measures, S, T, out_dtype=np.float32):

@@ -115,6 +115,22 @@ ocipError ocip_API ocipGetProximityBatchInfo(ocipProgram Program, int TemplateWi
                                              int TemplateHeight, int* NbItems,
                                              int* BandHeight);
 
+/* Best match of a template in one call (no reference counterpart).
+ * Computes the Measure (an ocipMeasure value) map of (Source, Template) and
+ * its index reduction IndexOp (0: ocipMinIndx, 1: ocipMaxIndx,
+ * 2: ocipMinAbsIndx, 3: ocipMaxAbsIndx), with the same answer as those calls
+ * on the map, ties included: the smallest (or largest) value and its (X, Y).
+ * One channel; Dest, when given, is F32 of the source's size and receives the
+ * map; it may be NULL. On the tensor path (templates up to 64 x 64) the
+ * reduction runs in the scoring kernel's epilogue, so without Dest no map is
+ * written at all. A map that holds a NaN (a _Norm measure over a zero-energy
+ * window) is reduced from the written map instead, because the reference's
+ * answer then depends on where the NaNs lie; the plain path and other shapes
+ * also compute the map (into Dest, or scratch) and reduce it. Synchronous. */
+ocipError ocip_API ocipProximityIndx(int Measure, int IndexOp, ocipImage Source,
+                                     ocipImage Template, ocipImage Dest, double* Value,
+                                     int* X, int* Y);
+
 /* Gradients of template matching (no reference counterpart).
  * For L = sum_{x,y} GradSqrDistance(x,y) * SqrDistance(Source, Template)(x,y)
  *       + sum_{x,y} GradCrossCorrNorm(x,y) * CrossCorr_Norm(Source, Template)(x,y)

@@ -34,7 +34,10 @@ struct Context {
     kEnergyMap = 4,      // row energies of the tensor path
     kProductMap = 5,     // F64 product sums of templates tiled over launches
     kTemplateStats = 6,  // per-channel template energy (FP64)
-    kNumScratch = 7
+    kIndexRecords = 7,   // per-warp best-match records of the fused reduction
+    kIndexMap = 8,       // score map of ocipProximityIndx when no Dest is given
+    kIndexScratch = 9,   // group results of the map-path index reduction
+    kNumScratch = 10
   };
   int device = 0;
   int sm_count = 0;

@@ -342,10 +342,102 @@ void index_op(int op, ocipProgram hp, ocipImage hs, double* result, int* x, int*
   ctx.check_device_errors();
 }
 
+// Best match in one call (extension): the measure, then the reference's
+// index reduction of its map. On the tensor path the reduction is fused into
+// the scoring epilogue and no map needs to be written; a NaN score (the
+// reference's answer then depends on where it lies) or a shape the fused
+// kernel does not take uses the written map and the reference-order
+// reduction.
+void proximity_index(int measure, int op, ocipImage hs, ocipImage ht, ocipImage hd,
+                     double* value, int* x, int* y) {
+  Context& ctx = current();
+  if (measure < kSqrDistance || measure > kCrossCorrNorm) fail(CL_INVALID_VALUE, "unknown measure");
+  if (op < kIdxMin || op > kIdxMaxAbs) fail(CL_INVALID_VALUE, "unknown index reduction");
+  if (value == nullptr || x == nullptr || y == nullptr) fail(CL_INVALID_VALUE, "NULL result");
+  Image& S = image(hs);
+  Image& T = image(ht);
+  Image* D = hd ? &image(hd) : nullptr;
+  same_context(ctx, S);
+  same_context(ctx, T);
+  if (D) same_context(ctx, *D);
+  if (T.desc.Width > S.desc.Width || T.desc.Height > S.desc.Height)
+    fail(CL_INVALID_VALUE, "Template image must be smaller than the source image.");
+  if (!same_type(S, T)) fail(CL_INVALID_VALUE, "Source and Template must have same type.");
+  if (S.desc.Channels > 1) fail(CL_INVALID_VALUE, "only 1 channel images are allowed");
+  if (D && (S.desc.Width != D->desc.Width || S.desc.Height != D->desc.Height))
+    fail(CL_INVALID_IMAGE_SIZE, "Different image sizes used");
+  if (D && (D->desc.Type != SImage::F32 || D->desc.Channels != 1))
+    fail(CL_INVALID_VALUE, "Dest of ocipProximityIndx must be F32 with one channel");
+  send_if_needed(S);
+  send_if_needed(T);
+  const Measure m = static_cast<Measure>(measure);
+  const DevImage s = dev_view(S), t = dev_view(T);
+  DevImage d;
+  if (D) {
+    d = dev_view(*D);
+  } else {
+    d.ptr = nullptr;
+    d.pitch = 0;
+    d.width = s.width;
+    d.height = s.height;
+    d.nch = 1;
+    d.type = F32;
+  }
+  const bool fused = ctx.path != OCIP_PATH_PLAIN && t.width <= 64 && t.height <= 64 &&
+                     tensor_supports(m, s, t, d, ctx.path == OCIP_PATH_TENSOR);
+  bool wrote_map = false;
+  if (fused) {
+    void* rec = ctx.scratch(Context::kIndexRecords, tensor_index_records_bytes(ctx, s, t));
+    int nrec = 0, bx = 0, by = 0;
+    float best = 0.f;
+    bool nan = false;
+    check_cuda(launch_proximity_tensor_indexed(ctx, m, s, t, d, op, rec, &nrec, &best, &bx, &by,
+                                               &nan),
+               "fused best-match launch");
+    ctx.last_path = OCIP_PATH_TENSOR;
+    if (D) mark_written(*D);
+    ctx.check_device_errors();
+    if (!nan) {
+      *value = best;
+      *x = bx;
+      *y = by;
+      return;
+    }
+    wrote_map = D != nullptr;
+  }
+  // The map path: the measure's map (Dest, or scratch), then the reduction.
+  DevImage map = d;
+  if (!D) {
+    map.pitch = ((size_t)s.width * 4 + 127) / 128 * 128;
+    map.ptr = ctx.scratch(Context::kIndexMap, map.pitch * s.height);
+  }
+  if (!wrote_map) {
+    cudaError_t e;
+    if (ctx.path != OCIP_PATH_PLAIN && tensor_supports(m, s, t, map, ctx.path == OCIP_PATH_TENSOR)) {
+      e = launch_proximity_tensor(ctx, m, s, t, map);
+      ctx.last_path = OCIP_PATH_TENSOR;
+    } else {
+      void* tt = ctx.scratch(Context::kTemplateEnergy, 64);
+      e = launch_proximity_plain(m, s, t, map, tt, ctx.stream);
+      ctx.last_path = OCIP_PATH_PLAIN;
+    }
+    check_cuda(e, "proximity kernel launch");
+    if (D) mark_written(*D);
+  }
+  void* scratch = ctx.scratch(Context::kIndexScratch, index_reduce_scratch_bytes(s.width, s.height));
+  check_cuda(index_reduce(ctx, op, map, scratch, value, x, y), "index reduction");
+  ctx.check_device_errors();
+}
+
 }  // namespace
 }  // namespace ocipb
 
 extern "C" {
+
+ocipError ocipProximityIndx(int Measure, int IndexOp, ocipImage Source, ocipImage Template,
+                            ocipImage Dest, double* Value, int* X, int* Y) {
+  OCIP_GUARD(proximity_index(Measure, IndexOp, Source, Template, Dest, Value, X, Y))
+}
 
 ocipError ocipPrepareStatistics(ocipProgram* ProgramPtr, ocipImage Img) {
   OCIP_GUARD(

@@ -196,6 +196,29 @@ struct ItemArgs {
   // 1: add the scores (raw CrossCorr sums into an F64 map) to the
   // destination instead of writing them (templates tiled over launches).
   int accum;
+  // Best match (ocipProximityIndx): -1 none, else the index reduction
+  // (0 min, 1 max, 2 min |v|, 3 max |v|) of the F32 scores; each epilogue
+  // warp writes one IdxRecord per item to idx_out[item * 4 + warp]. dst may
+  // then be null (no map written).
+  int idx_op;
+  char* idx_out;
+};
+
+// Best score of an epilogue warp's positions in one item. Among equal values
+// the smallest key wins: key = (reference work-group index << 12) |
+// (bit-reversed work-item id << 4) | pixel index within the work-item, the
+// order in which the reference's index reduction resolves ties
+// (cl-files/Statistics.cl REDUCE_POS: a strict scan of 16 pixels per
+// work-item, a tree fold over work-items that keeps the left one on ties, a
+// strict fold over work-groups). NaN scores are only flagged: with a NaN in
+// the map the reference's answer depends on where it lies, so the caller
+// takes the map path then.
+struct IdxRecord {
+  float v;
+  int have;
+  unsigned long long key;
+  int nan;
+  int pad;
 };
 
 // Shared-memory layout, identical on host and device.
@@ -306,11 +329,42 @@ __device__ __forceinline__ bool builders_all(bool p) {
   return r != 0;
 }
 
+// Running best of one lane (the fused best match): the value, its key and
+// flags. A value replaces the best when strictly better, or equal with a
+// smaller key; NaN values are only flagged.
+struct IdxState {
+  float v;
+  unsigned long long key;
+  int have, nan;
+};
+
+__device__ __forceinline__ unsigned long long idx_key_of(int x, int y, int ngx) {
+  const unsigned lid = ((unsigned)(y & 15) << 4) | (unsigned)(x & 15);
+  const unsigned long long grp = (unsigned long long)(y >> 4) * ngx + (x >> 8);
+  return (grp << 12) | ((unsigned long long)(__brev(lid) >> 24) << 4) | (unsigned)((x & 255) >> 4);
+}
+
+__device__ __forceinline__ void idx_state_update(IdxState& st, float v, int x, int y, int op,
+                                                 int ngx) {
+  const float c = op >= 2 ? fabsf(v) : v;
+  if (c != c) {
+    st.nan = 1;
+    return;
+  }
+  const bool is_min = op == 0 || op == 2;
+  if (st.have && (is_min ? c > st.v : c < st.v)) return;
+  const unsigned long long k = idx_key_of(x, y, ngx);
+  if (st.have && c == st.v && k > st.key) return;
+  st.v = c;
+  st.key = k;
+  st.have = 1;
+}
+
 // Runs one work item with all 10 warps of the CTA. The caller has
 // synchronised the CTA; TMEM (512 columns) is allocated. Barriers are
 // initialised here and invalidated at the end, so consecutive items may use
 // different layouts.
-template <int ELEM, int S>
+template <int ELEM, int S, bool IDX>
 __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem, CtaState& cs) {
   typedef ElemTraits<ELEM> TR;
   constexpr bool SPLIT = TR::split;
@@ -549,6 +603,7 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     // the score loop would otherwise reload them on every slot.
     const auto ea_W = a.W;
     const auto ea_accum = a.accum;
+    const int ea_idx_op = IDX ? a.idx_op : -1;
     const auto ea_dst = a.dst;
     const auto ea_dst_f64 = a.dst_f64;
     const auto ea_dst_pitch = a.dst_pitch;
@@ -564,6 +619,14 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
     // numerator is formed in FP64; the _Norm scale of an F32 map is taken in
     // FP32 (relative error a few 1e-7), of an F64 map in FP64. U8: exact
     // integers and the plain path's float or double formulas (bit-identical).
+    // Best-match state of this lane (ocipProximityIndx).
+    IdxState ib;
+    ib.v = 0.f;
+    ib.key = 0ull;
+    ib.have = 0;
+    ib.nan = 0;
+    const int idx_ngx = (ea_W + 255) >> 8;
+    auto idx_update = [&](float v, int x, int y) { idx_state_update(ib, v, x, y, ea_idx_op, idx_ngx); };
     // U8 _Norm: float arithmetic where the plain path's float sums are exact.
     const bool u8_float = (double)a.tw * a.th * 65025.0 <= 16777216.0;
     // Scores with the measure fixed at compile time (MT::value), so that the
@@ -725,17 +788,24 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
               float outf[S];
 #pragma unroll
               for (int p = 0; p < S; ++p) outf[p] = score_f(mt, val[g * S + p], e[p]);
-              float* o = reinterpret_cast<float*>(orow) + x0;
-              if (S % 4 == 0) {
+              if (IDX && ea_idx_op >= 0) {
 #pragma unroll
-                for (int j = 0; j < S / 4; ++j)
-                  reinterpret_cast<float4*>(o)[j] = make_float4(
-                      outf[(4 * j) % S], outf[(4 * j + 1) % S], outf[(4 * j + 2) % S],
-                      outf[(4 * j + 3) % S]);
-              } else {
+                for (int p = 0; p < S; ++p) idx_update(outf[p], x0 + p, yd);
+              }
+              if (ea_dst != nullptr) {
+                float* o = reinterpret_cast<float*>(orow) + x0;
+                if (S % 4 == 0) {
 #pragma unroll
-                for (int j = 0; j < S / 2; ++j)
-                  reinterpret_cast<float2*>(o)[j] = make_float2(outf[(2 * j) % S], outf[(2 * j + 1) % S]);
+                  for (int j = 0; j < S / 4; ++j)
+                    reinterpret_cast<float4*>(o)[j] = make_float4(
+                        outf[(4 * j) % S], outf[(4 * j + 1) % S], outf[(4 * j + 2) % S],
+                        outf[(4 * j + 3) % S]);
+                } else {
+#pragma unroll
+                  for (int j = 0; j < S / 2; ++j)
+                    reinterpret_cast<float2*>(o)[j] =
+                        make_float2(outf[(2 * j) % S], outf[(2 * j + 1) % S]);
+                }
               }
             } else {
 #pragma unroll
@@ -743,12 +813,15 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
                 const int x = x0 + p;
                 if (x >= ea_W) break;
                 const size_t xo = (size_t)x * ea_nch + ch;
-                if (ea_dst_f64 && ea_accum)
+                if (ea_dst_f64 && ea_accum) {
                   reinterpret_cast<double*>(orow)[xo] += score_d(mt, val[g * S + p], e[p]);
-                else if (ea_dst_f64)
+                } else if (ea_dst_f64) {
                   reinterpret_cast<double*>(orow)[xo] = score_d(mt, val[g * S + p], e[p]);
-                else
-                  reinterpret_cast<float*>(orow)[xo] = score_f(mt, val[g * S + p], e[p]);
+                } else {
+                  const float v = score_f(mt, val[g * S + p], e[p]);
+                  if (IDX && ea_idx_op >= 0) idx_update(v, x, yd);
+                  if (ea_dst != nullptr) reinterpret_cast<float*>(orow)[xo] = v;
+                }
               }
             }
           }
@@ -761,6 +834,34 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         default: slots(std::integral_constant<int, kCrossCorr>()); break;
       }
       if (!__all_sync(0xffffffffu, ok)) break;
+    }
+    if (IDX && ea_idx_op >= 0) {
+      // The warp's best: same rule, then lane 0 writes the warp's record.
+      const bool is_min = ea_idx_op == 0 || ea_idx_op == 2;
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, ib.v, d);
+        const unsigned long long ok2 = __shfl_xor_sync(0xffffffffu, ib.key, d);
+        const int oh = __shfl_xor_sync(0xffffffffu, ib.have, d);
+        ib.nan |= __shfl_xor_sync(0xffffffffu, ib.nan, d);
+        const bool take = oh && (!ib.have || (is_min ? ov < ib.v : ov > ib.v) ||
+                                 (ov == ib.v && ok2 < ib.key));
+        if (take) {
+          ib.v = ov;
+          ib.key = ok2;
+          ib.have = 1;
+        }
+      }
+      if (lane == 0) {
+        const int item = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        IdxRecord r;
+        r.v = ib.v;
+        r.have = ib.have;
+        r.key = ib.key;
+        r.nan = ib.nan;
+        r.pad = 0;
+        reinterpret_cast<IdxRecord*>(a.idx_out)[item * kEpilogue + sp] = r;
+      }
     }
   }
 
@@ -790,14 +891,14 @@ int strip_width(int cls) {
   return kM * s_for(class_r(cls));
 }
 
-template <int ELEM>
+template <int ELEM, bool IDX>
 __device__ __forceinline__ void dispatch(const ItemArgs& a, unsigned char* smem, CtaState& cs) {
   if (a.R == 16)
-    run_item<ELEM, 8>(a, smem, cs);
+    run_item<ELEM, 8, IDX>(a, smem, cs);
   else if (a.R == 32)
-    run_item<ELEM, 4>(a, smem, cs);
+    run_item<ELEM, 4, IDX>(a, smem, cs);
   else
-    run_item<ELEM, 2>(a, smem, cs);
+    run_item<ELEM, 2, IDX>(a, smem, cs);
 }
 
 // Batch tables (device memory).
@@ -848,7 +949,7 @@ struct TensorLaunch {
 // One kernel per element type. Mode 0 (one image and template): CTA
 // (x, y, z) = (strip, band, channel). Mode 1 (batch): one persistent CTA per
 // SM takes items from a global counter until none are left.
-template <int ELEM>
+template <int ELEM, bool IDX = false>
 __global__ void __launch_bounds__(kThreads, 1)
     prox_tensor_kernel(const __grid_constant__ TensorLaunch P) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -873,7 +974,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       item.yend = min(item.H, item.y0 + P.BH);
     }
     __syncthreads();
-    dispatch<ELEM>(item, smem, cs);
+    dispatch<ELEM, IDX>(item, smem, cs);
   } else {
     for (;;) {
       if (threadIdx.x == 0) {
@@ -905,6 +1006,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           item.dst_f64 = ds.f64;
           item.measure = P.measure;
           item.accum = 0;
+          item.idx_op = -1;
+          item.idx_out = nullptr;
           item.energy = nullptr;
           item.e_pitch = item.e_plane = 0;
           if (bi.energy >= 0) {
@@ -918,7 +1021,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncthreads();
       const int it = cs.next;
       if (it >= P.nitems) break;
-      dispatch<ELEM>(item, smem, cs);
+      dispatch<ELEM, IDX>(item, smem, cs);
       __syncthreads();  // every thread has read the item before it is replaced
     }
   }
@@ -1063,7 +1166,8 @@ size_t plane_set_bytes(const DevImage& s) {
 
 template <int ELEM>
 cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevImage& tmpl,
-                       const DevImage& dst, int ax, int ay, bool accum = false) {
+                       const DevImage& dst, int ax, int ay, bool accum = false,
+                       int idx_op = -1, void* idx_out = nullptr, int* nrec = nullptr) {
   const int cls = class_of(tmpl.height);
   const int R = class_r(cls);
   TensorLaunch P;
@@ -1094,6 +1198,8 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
   a.dst_f64 = dst.type == F64;
   a.measure = m;
   a.accum = accum ? 1 : 0;
+  a.idx_op = idx_op;
+  a.idx_out = reinterpret_cast<char*>(idx_out);
 
   const int smem_bytes = smem_for<ELEM>(cls, tmpl.width, ax, P.nbox);
   if (smem_bytes > kMaxDynSmem) return cudaErrorInvalidValue;
@@ -1122,11 +1228,12 @@ cudaError_t launch_one(Context& ctx, Measure m, const DevImage& src, const DevIm
                                       plane_pitch, plane_pitch * src.height, P.nbox);
   if (e != cudaSuccess) return e;
 
-  auto kern = prox_tensor_kernel<ELEM>;
+  auto kern = idx_op >= 0 ? prox_tensor_kernel<ELEM, true> : prox_tensor_kernel<ELEM, false>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            kMaxDynSmem);
   if (e != cudaSuccess) return e;
   dim3 grid(nstrips, (src.height + P.BH - 1) / P.BH, src.nch);
+  if (nrec) *nrec = (int)(grid.x * grid.y * grid.z) * kEpilogue;
   kern<<<grid, kThreads, smem_bytes, ctx.stream>>>(P);
   count_launches(1);
   return cudaGetLastError();
@@ -1585,6 +1692,62 @@ cudaError_t launch_proximity_tensor_anchored(Context& ctx, Measure m, const DevI
   if (src.type == U8) return launch_one<kU8>(ctx, m, src, tmpl, dst, ax, ay);
   if (src.type == U16) return launch_one<kU16>(ctx, m, src, tmpl, dst, ax, ay);
   return launch_one<kF32>(ctx, m, src, tmpl, dst, ax, ay);
+}
+
+size_t tensor_index_records_bytes(const Context& ctx, const DevImage& src, const DevImage& tmpl) {
+  (void)ctx;
+  const int cls = class_of(tmpl.height);
+  const int sw = kM * s_for(class_r(cls));
+  const size_t nstrips = (src.width + sw - 1) / sw;
+  // At most one band per row (a fixed band height of 1).
+  const size_t nbands = src.height;
+  return nstrips * nbands * src.nch * kEpilogue * sizeof(IdxRecord);
+}
+
+cudaError_t launch_proximity_tensor_indexed(Context& ctx, Measure m, const DevImage& src,
+                                            const DevImage& tmpl, const DevImage& dst, int idx_op,
+                                            void* records, int* nrec, float* best, int* bx,
+                                            int* by, bool* has_nan) {
+  cudaError_t e;
+  const int ax = tmpl.width / 2, ay = tmpl.height / 2;
+  if (src.type == U8)
+    e = launch_one<kU8>(ctx, m, src, tmpl, dst, ax, ay, false, idx_op, records, nrec);
+  else if (src.type == U16)
+    e = launch_one<kU16>(ctx, m, src, tmpl, dst, ax, ay, false, idx_op, records, nrec);
+  else
+    e = launch_one<kF32>(ctx, m, src, tmpl, dst, ax, ay, false, idx_op, records, nrec);
+  if (e != cudaSuccess) return e;
+  std::vector<IdxRecord> recs(*nrec);
+  e = cudaMemcpyAsync(recs.data(), records, recs.size() * sizeof(IdxRecord),
+                      cudaMemcpyDeviceToHost, ctx.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(ctx.stream);
+  if (e != cudaSuccess) return e;
+  const bool is_min = idx_op == 0 || idx_op == 2;
+  bool have = false, nan = false;
+  float v = 0.f;
+  unsigned long long key = 0;
+  for (const IdxRecord& r : recs) {
+    nan = nan || r.nan;
+    if (!r.have) continue;
+    if (!have || (is_min ? r.v < v : r.v > v) || (r.v == v && r.key < key)) {
+      v = r.v;
+      key = r.key;
+      have = true;
+    }
+  }
+  *has_nan = nan;
+  *best = v;
+  // Key -> pixel: group, bit-reversed work-item id, pixel index in the work-item.
+  const unsigned long long grp = key >> 12;
+  const unsigned rl = (unsigned)((key >> 4) & 255);  // bit-reversed work-item id
+  unsigned lid = 0;
+  for (int b = 0; b < 8; ++b) lid |= ((rl >> b) & 1u) << (7 - b);
+  const int i = (int)(key & 15);
+  const int ngx = (src.width + 255) >> 8;
+  *bx = (int)(grp % ngx) * 256 + (int)(lid & 15) + 16 * i;
+  *by = (int)(grp / ngx) * 16 + (int)(lid >> 4);
+  return have ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_tensor_product_sums(Context& ctx, const DevImage& src, const DevImage& tmpl,

@@ -39,6 +39,19 @@ cudaError_t launch_tensor_product_sums(Context& ctx, const DevImage& src, const 
 cudaError_t launch_proximity_tensor_large(Context& ctx, Measure m, const DevImage& src,
                                           const DevImage& tmpl, const DevImage& dst);
 
+// Best match of a one-channel F32 score map on the tensor path, fused into the
+// scoring epilogue (ocipProximityIndx): the index reduction idx_op (0 min,
+// 1 max, 2 min |v|, 3 max |v|) of the F32 scores, with the reference's tie
+// order. dst may have a null pointer (no map written). records is device
+// scratch of tensor_index_records_bytes() bytes. Synchronises the stream;
+// *has_nan reports a NaN score (the caller then reduces a written map, whose
+// answer depends on where the NaNs lie).
+size_t tensor_index_records_bytes(const Context& ctx, const DevImage& src, const DevImage& tmpl);
+cudaError_t launch_proximity_tensor_indexed(Context& ctx, Measure m, const DevImage& src,
+                                            const DevImage& tmpl, const DevImage& dst, int idx_op,
+                                            void* records, int* nrec, float* best, int* bx,
+                                            int* by, bool* has_nan);
+
 // Gradients of L = sum G1 * SqrDistance(S, T) + sum G2 * CrossCorr_Norm(S, T)
 // (F32 sources, one channel, templates up to 64 x 64) into dS (S's size) and
 // dT (T's size), F32 or F64; G1 or G2 may be null, N2 is CrossCorr_Norm(S, T)

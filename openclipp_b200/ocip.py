@@ -95,6 +95,9 @@ def _load():
         "ocipGetStream": (i32, [ctypes.POINTER(vp)]),
         "ocipGetImageDevicePtr": (i32, [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t)]),
         "ocipGetLaunchCount": (i32, [ctypes.POINTER(ctypes.c_uint64)]),
+        "ocipProximityIndx": (i32, [ctypes.c_int, ctypes.c_int, vp, vp, vp,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int)]),
         "ocipIntegralNoAlloc": (i32, [ctypes.c_int, SImage, vp, ctypes.c_size_t, SImage, vp,
                                       ctypes.c_size_t, vp]),
         "ocipPrepareProximityBatch": (i32, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp),
@@ -351,6 +354,21 @@ def proximity_backward(S, T, G1=None, G2=None, N2=None, dS=None, dT=None):
     the error code."""
     h = lambda x: x.handle if x is not None else None
     return lib.ocipProximityBackward(h(S), h(T), h(G1), h(G2), h(N2), h(dS), h(dT))
+
+
+INDEX_OPS = {"MinIndx": 0, "MaxIndx": 1, "MinAbsIndx": 2, "MaxAbsIndx": 3}
+
+
+def proximity_index(measure, op, S, T, D=None):
+    """ocipProximityIndx: (error code, value, x, y) of the index reduction `op`
+    (MinIndx, MaxIndx, MinAbsIndx, MaxAbsIndx) of the measure's map; D, when
+    given, receives the map."""
+    v, x, y = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    code = measure if isinstance(measure, int) else MEASURE_INDEX[measure]
+    rc = lib.ocipProximityIndx(code, INDEX_OPS[op], S.handle, T.handle,
+                               D.handle if D is not None else None, ctypes.byref(v),
+                               ctypes.byref(x), ctypes.byref(y))
+    return rc, v.value, x.value, y.value
 
 
 def prepare_statistics(img=None):
