@@ -24,8 +24,14 @@
 // Shared-memory rows are stored in 16-byte chunks with one pad chunk after
 // every 8, so the lanes' stride-2 (float) or stride-4 (double) chunk accesses
 // hit distinct banks. Very tall templates are processed in row bands.
+//
+// F32 AbsDistance, the one measure without a tensor-core form, runs on
+// sm_100's packed FP32 adds over pairs of output rows (PackedAbs below),
+// specialised on the width of the template's last column chunk so that the
+// inner loop has no bounds tests.
 #include <algorithm>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -95,6 +101,20 @@ __host__ __device__ inline int row_bytes_for(int L) {
   return (chunks + chunks / 8 + 1) * 16;
 }
 
+// Packed FP32 AbsDistance. Output rows 2jp and 2jp + 1 of one column meet
+// the same source element at every step (their template rows are h and
+// h - 1), so the template is staged as negated row pairs (-t(h, w),
+// -t(h - 1, w)) and one sm_100 packed add (__fadd2_rn) forms both rows'
+// differences, s + (-t) being s - t exactly (IEEE subtraction is the addition
+// of the negation); a second packed add folds their absolute values into the
+// two rows' sums. Every per-output operation and its order are the scalar
+// form's, so the results are bit-identical; the packed adds halve the
+// instructions and, unlike scalar adds, load both halves of the FP32 pipe.
+template <int TYPE, int MEAS>
+struct PackedAbs {
+  static constexpr bool value = TYPE == F32 && MEAS == kAbsDistance;
+};
+
 // One template-column chunk applied to one output row.
 template <typename CT, int MEAS>
 __device__ __forceinline__ void apply_chunk(CT (&acc)[RX], CT (&acc2)[RX],
@@ -127,11 +147,14 @@ __device__ __forceinline__ void apply_chunk(CT (&acc)[RX], CT (&acc2)[RX],
   }
 }
 
-template <int TYPE, typename CT, int MEAS, int RY>
+// KT: for the packed FP32 AbsDistance form, the columns of the template's last
+// chunk, tw - WCH * ((tw - 1) / WCH), in 1 .. WCH; 0 for the other forms.
+template <int TYPE, typename CT, int MEAS, int RY, int KT>
 __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     prox_plain_kernel(const PlainParams p) {
   using ET = typename ElemOf<TYPE>::T;
   constexpr bool kNorm = (MEAS == kCrossCorrNorm || MEAS == kSqrDistanceNorm);
+  constexpr bool kPackedAbs = PackedAbs<TYPE, MEAS>::value;
   constexpr int TY = kWarps * RY;
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* s_src = smem;
@@ -147,9 +170,15 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
   const int L = TX + p.twp;          // logical elements per source row
   const int qtot = TY + p.th - 1;    // source rows needed by the tile
   const int nwc = p.twp / WCH;
+  const int tstride = kPackedAbs ? 2 * p.twp : p.twp;  // template row stride in s_t
 
   CT acc[RY][RX];
   CT acc2[RY][RX];
+  float2 accr[RY / 2][RX];  // packed AbsDistance: output rows (2jp, 2jp + 1) of column i
+#pragma unroll
+  for (int j = 0; j < RY / 2; ++j)
+#pragma unroll
+    for (int i = 0; i < RX; ++i) accr[j][i] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int j = 0; j < RY; ++j)
 #pragma unroll
@@ -165,82 +194,205 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     const int tg0 = max(0, g0 - (TY - 1));
     const int tg1 = min(p.th, g1);
     if (band > 0) __syncthreads();
-    // Stage source rows [g0, g1) x logical columns [0, L).
-    const int nel = (g1 - g0) * L;
-    for (int idx = threadIdx.x; idx < nel; idx += kThreads) {
-      const int q = idx / L;
-      const int e = idx - q * L;
-      const int gy = y0 + top + g0 + q;
-      const int gx = x0 + left + e;
-      CT v = CT(0);
-      if (gx >= 0 && gx < p.W && gy >= 0 && gy < p.H)
-        v = (CT)(*reinterpret_cast<const ET*>(
-            p.src + (size_t)gy * p.src_pitch + ((size_t)gx * p.nch + c) * sizeof(ET)));
-      *reinterpret_cast<CT*>(s_src + (size_t)q * p.rowBytes + phys_off<CT>(e)) = v;
+    // Stage source rows [g0, g1) x logical columns [0, L): a warp per row,
+    // lanes along the row (coalesced), zero outside the image. Sources of the
+    // compute type are copied asynchronously (no register round trip), the
+    // copies overlapping the template staging below.
+    for (int qq = warp; qq < g1 - g0; qq += kWarps) {
+      const int gy = y0 + top + g0 + qq;
+      const bool row_in = gy >= 0 && gy < p.H;
+      const ET* grow =
+          reinterpret_cast<const ET*>(p.src + (size_t)(row_in ? gy : 0) * p.src_pitch) + c;
+      unsigned char* srow = s_src + (size_t)qq * p.rowBytes;
+      if constexpr (std::is_same<CT, ET>::value) {
+        // Asynchronous copies, zero-filled outside the image (source size 0).
+#pragma unroll 4
+        for (int e = lane; e < L; e += 32) {
+          const int gx = x0 + left + e;
+          const bool in = row_in && gx >= 0 && gx < p.W;
+          const ET* g = grow + (size_t)(in ? gx : 0) * p.nch;
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(srow + phys_off<CT>(e));
+          asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(g),
+                       "n"((int)sizeof(ET)), "r"(in ? (int)sizeof(ET) : 0)
+                       : "memory");
+        }
+      } else {
+#pragma unroll 4
+        for (int e = lane; e < L; e += 32) {
+          const int gx = x0 + left + e;
+          CT v = CT(0);
+          if (row_in && gx >= 0 && gx < p.W) v = (CT)grow[(size_t)gx * p.nch];
+          *reinterpret_cast<CT*>(srow + phys_off<CT>(e)) = v;
+        }
+      }
     }
-    // Stage template rows [tg0, tg1), zero-padded to twp columns.
-    const int ntel = (tg1 - tg0) * p.twp;
+    if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // Stage template rows [tg0, tg1), zero-padded to twp columns. The packed
+    // AbsDistance form stores row h as the negated pairs (t(h, w), t(h - 1, w)).
+    const int ntel = (tg1 - tg0) * tstride;
     for (int idx = threadIdx.x; idx < ntel; idx += kThreads) {
-      const int hh = idx / p.twp;
-      const int w = idx - hh * p.twp;
+      const int hh = idx / tstride;
+      int w = idx - hh * tstride;
+      int trow = tg0 + hh;
+      if (kPackedAbs) {  // pairs (row h, row h - 1) of column w
+        w = (idx - hh * tstride) >> 1;
+        trow -= (idx - hh * tstride) & 1;
+      }
       CT v = CT(0);
-      if (w < p.tw)
+      if (w < p.tw && trow >= 0)
         v = (CT)(*reinterpret_cast<const ET*>(
-            p.tmpl + (size_t)(tg0 + hh) * p.tmpl_pitch + ((size_t)w * p.nch + c) * sizeof(ET)));
-      s_t[idx] = v;
+            p.tmpl + (size_t)trow * p.tmpl_pitch + ((size_t)w * p.nch + c) * sizeof(ET)));
+      s_t[idx] = kPackedAbs ? -v : v;
     }
+    if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
 
+    // Window of source row q for template columns wc*WCH ..: RX + WCH elements.
+    auto load_window = [&](const unsigned char* srow, int wc, CT (&win)[RX + WCH]) {
+      const int e0 = lane * RX + wc * WCH;
+      constexpr int E = 16 / sizeof(CT);
+#pragma unroll
+      for (int v = 0; v < (RX + WCH) / E; ++v) {
+        const int e = e0 + v * E;
+        if (sizeof(CT) == 4) {
+          const float4 f = *reinterpret_cast<const float4*>(srow + phys_off<CT>(e));
+          win[v * 4 + 0] = (CT)f.x;
+          win[v * 4 + 1] = (CT)f.y;
+          win[v * 4 + 2] = (CT)f.z;
+          win[v * 4 + 3] = (CT)f.w;
+        } else {
+          const double2 d = *reinterpret_cast<const double2*>(srow + phys_off<CT>(e));
+          win[v * 2 + 0] = (CT)d.x;
+          win[v * 2 + 1] = (CT)d.y;
+        }
+      }
+    };
+    auto load_tmpl = [&](const CT* trow, CT (&tv)[WCH]) {
+      if (sizeof(CT) == 4) {
+        const float4 a = reinterpret_cast<const float4*>(trow)[0];
+        const float4 b = reinterpret_cast<const float4*>(trow)[1];
+        tv[0] = (CT)a.x; tv[1] = (CT)a.y; tv[2] = (CT)a.z; tv[3] = (CT)a.w;
+        tv[4] = (CT)b.x; tv[5] = (CT)b.y; tv[6] = (CT)b.z; tv[7] = (CT)b.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < WCH / 2; ++k) {
+          const double2 d = reinterpret_cast<const double2*>(trow)[k];
+          tv[2 * k] = (CT)d.x;
+          tv[2 * k + 1] = (CT)d.y;
+        }
+      }
+    };
+
+    // Source rows q meet template rows h = q - warp*RY - j of the warp's
+    // output rows j. Rows where some h falls outside the template (the first
+    // and last RY - 1 of the warp) take the checked loop; the others, where
+    // every output row has a template row, take the unchecked one.
     const int qa = max(g0, warp * RY);
     const int qb = min(g1, warp * RY + RY + p.th - 1);
-    for (int q = qa; q < qb; ++q) {
+    const int lo = min(max(qa, warp * RY + RY - 1), qb);
+    const int hi = min(max(lo, warp * RY + p.th), qb);
+    auto row_checked = [&](int q) {
       const int r = q - warp * RY;
       const unsigned char* srow = s_src + (size_t)(q - g0) * p.rowBytes;
       for (int wc = 0; wc < nwc; ++wc) {
         CT win[RX + WCH];
-        const int e0 = lane * RX + wc * WCH;
-        constexpr int E = 16 / sizeof(CT);
-#pragma unroll
-        for (int v = 0; v < (RX + WCH) / E; ++v) {
-          const int e = e0 + v * E;
-          if (sizeof(CT) == 4) {
-            const float4 f = *reinterpret_cast<const float4*>(srow + phys_off<CT>(e));
-            win[v * 4 + 0] = (CT)f.x;
-            win[v * 4 + 1] = (CT)f.y;
-            win[v * 4 + 2] = (CT)f.z;
-            win[v * 4 + 3] = (CT)f.w;
-          } else {
-            const double2 d = *reinterpret_cast<const double2*>(srow + phys_off<CT>(e));
-            win[v * 2 + 0] = (CT)d.x;
-            win[v * 2 + 1] = (CT)d.y;
-          }
-        }
+        load_window(srow, wc, win);
         const int kmax = min(WCH, p.tw - wc * WCH);
 #pragma unroll
         for (int j = 0; j < RY; ++j) {
           const int h = r - j;
           if (h < 0 || h >= p.th) continue;
-          const CT* trow = s_t + (size_t)(h - tg0) * p.twp + wc * WCH;
           CT tv[WCH];
-          if (sizeof(CT) == 4) {
-            const float4 a = reinterpret_cast<const float4*>(trow)[0];
-            const float4 b = reinterpret_cast<const float4*>(trow)[1];
-            tv[0] = (CT)a.x; tv[1] = (CT)a.y; tv[2] = (CT)a.z; tv[3] = (CT)a.w;
-            tv[4] = (CT)b.x; tv[5] = (CT)b.y; tv[6] = (CT)b.z; tv[7] = (CT)b.w;
-          } else {
-#pragma unroll
-            for (int k = 0; k < WCH / 2; ++k) {
-              const double2 d = reinterpret_cast<const double2*>(trow)[k];
-              tv[2 * k] = (CT)d.x;
-              tv[2 * k + 1] = (CT)d.y;
-            }
-          }
+          load_tmpl(s_t + (size_t)(h - tg0) * tstride + wc * WCH, tv);
           if (kmax == WCH)
             apply_chunk<CT, MEAS>(acc[j], acc2[j], win, tv, WCH);
           else
             apply_chunk<CT, MEAS>(acc[j], acc2[j], win, tv, kmax);
         }
       }
+    };
+    if constexpr (kPackedAbs) {
+      // Chunks of WCH template columns: nfull full ones, then the last, of
+      // KT columns. check: some of the rows' template rows may lie outside.
+      const int nfull = (p.tw - 1) / WCH;
+      auto rows = [&](int qbeg, int qend, auto check) {
+        for (int q = qbeg; q < qend; ++q) {
+          const unsigned char* srow = s_src + (size_t)(q - g0) * p.rowBytes;
+          const CT* t0 = s_t + (size_t)(q - warp * RY - tg0) * tstride;
+          auto chunk = [&](int wc, auto kmaxc) {
+            constexpr int KMAX = decltype(kmaxc)::value;
+            CT win[RX + WCH];
+            load_window(srow, wc, win);
+            float2 sd[RX + WCH];  // each window element in both halves
+#pragma unroll
+            for (int e = 0; e < RX + WCH; ++e) sd[e] = make_float2(win[e], win[e]);
+#pragma unroll
+            for (int jp = 0; jp < RY / 2; ++jp) {
+              // Rows near the warp's first and last source rows: a pair whose
+              // template rows are both inside the template is packed, a pair
+              // with one inside takes only that half (scalar), else none.
+              int both = 3;
+              if (decltype(check)::value) {
+                const int h = q - warp * RY - 2 * jp;
+                both = (h >= 0 && h < p.th ? 1 : 0) | (h >= 1 && h - 1 < p.th ? 2 : 0);
+              }
+              if (both == 3) {
+                const float4* tr =
+                    reinterpret_cast<const float4*>(t0 - (size_t)(2 * jp) * tstride + 2 * wc * WCH);
+                float2 tp[WCH];  // (-t(h, k), -t(h - 1, k)), h the template row of output row 2jp
+#pragma unroll
+                for (int m = 0; m < WCH / 2; ++m) {
+                  const float4 f = tr[m];
+                  tp[2 * m] = make_float2(f.x, f.y);
+                  tp[2 * m + 1] = make_float2(f.z, f.w);
+                }
+#pragma unroll
+                for (int k = 0; k < KMAX; ++k) {
+#pragma unroll
+                  for (int i = 0; i < RX; ++i) {
+                    const float2 d = __fadd2_rn(sd[i + k], tp[k]);
+                    accr[jp][i] = __fadd2_rn(accr[jp][i], make_float2(fabsf(d.x), fabsf(d.y)));
+                  }
+                }
+              } else if (both != 0) {
+                // The one template row inside: h (output row 2jp) or h - 1
+                // (row 2jp + 1), read from its own staged row.
+                const float4* tr = reinterpret_cast<const float4*>(
+                    t0 - (size_t)(2 * jp + (both == 2 ? 1 : 0)) * tstride + 2 * wc * WCH);
+                float tv[WCH];
+#pragma unroll
+                for (int m = 0; m < WCH / 2; ++m) {
+                  const float4 f = tr[m];
+                  tv[2 * m] = f.x;
+                  tv[2 * m + 1] = f.z;
+                }
+                if (both == 1) {
+#pragma unroll
+                  for (int k = 0; k < KMAX; ++k)
+#pragma unroll
+                    for (int i = 0; i < RX; ++i)
+                      accr[jp][i].x = __fadd_rn(accr[jp][i].x, fabsf(__fadd_rn(win[i + k], tv[k])));
+                } else {
+#pragma unroll
+                  for (int k = 0; k < KMAX; ++k)
+#pragma unroll
+                    for (int i = 0; i < RX; ++i)
+                      accr[jp][i].y = __fadd_rn(accr[jp][i].y, fabsf(__fadd_rn(win[i + k], tv[k])));
+                }
+              }
+            }
+          };
+          for (int wc = 0; wc < nfull; ++wc) chunk(wc, std::integral_constant<int, WCH>());
+          chunk(nfull, std::integral_constant<int, KT>());
+        }
+      };
+      rows(qa, lo, std::true_type());
+      rows(lo, hi, std::false_type());
+      rows(hi, qb, std::true_type());
+    } else {
+      for (int q = qa; q < lo; ++q) row_checked(q);
+      for (int q = lo; q < hi; ++q) row_checked(q);
+      for (int q = hi; q < qb; ++q) row_checked(q);
     }
   }
 
@@ -256,6 +408,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
       const int x = x0 + lane * RX + i;
       if (x >= p.W) continue;
       CT v = acc[j][i];
+      if constexpr (kPackedAbs) v = (j & 1) ? accr[j / 2][i].y : accr[j / 2][i].x;
       if (kNorm) v = dv(v, sq(mul(acc2[j][i], tt)));
       char* o = p.dst + (size_t)y * p.dst_pitch;
       if (p.dst_f64)
@@ -324,7 +477,8 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
   int RB = qtot;
   auto bytes_for = [&](int rb) {
     const int tb = std::min(p.th, rb + TY - 1);
-    return (size_t)rb * p.rowBytes + (size_t)tb * p.twp * sizeof(CT);
+    return (size_t)rb * p.rowBytes +
+           (size_t)tb * p.twp * sizeof(CT) * (PackedAbs<TYPE, MEAS>::value ? 2 : 1);
   };
   while (RB > 1 && bytes_for(RB) > (size_t)kSmemBudget) RB = (RB + 1) / 2;
   if (bytes_for(RB) > (size_t)kSmemBudget) return cudaErrorInvalidValue;
@@ -339,7 +493,19 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
         (const char*)tmpl.ptr, tmpl.pitch, tmpl.nch, p.tw, p.th, (CT*)tt_buf);
     count_launches(1);
   }
-  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY>;
+  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY, PackedAbs<TYPE, MEAS>::value ? WCH : 0>;
+  if constexpr (PackedAbs<TYPE, MEAS>::value) {
+    switch (p.tw - WCH * ((p.tw - 1) / WCH)) {
+      case 1: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 1>; break;
+      case 2: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 2>; break;
+      case 3: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 3>; break;
+      case 4: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 4>; break;
+      case 5: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 5>; break;
+      case 6: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 6>; break;
+      case 7: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 7>; break;
+      default: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 8>; break;
+    }
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
