@@ -229,7 +229,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.commit_group;\n" ::: "memory");
     // Stage template rows [tg0, tg1), zero-padded to twp columns. The packed
     // AbsDistance form stores row h as the negated pairs (t(h, w), t(h - 1, w)).
+    // Read-only loads, unrolled, so that a thread's loads are in flight together.
     const int ntel = (tg1 - tg0) * tstride;
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < ntel; idx += kThreads) {
       const int hh = idx / tstride;
       int w = idx - hh * tstride;
@@ -240,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
       }
       CT v = CT(0);
       if (w < p.tw && trow >= 0)
-        v = (CT)(*reinterpret_cast<const ET*>(
+        v = (CT)__ldg(reinterpret_cast<const ET*>(
             p.tmpl + (size_t)trow * p.tmpl_pitch + ((size_t)w * p.nch + c) * sizeof(ET)));
       s_t[idx] = kPackedAbs ? -v : v;
     }
@@ -403,18 +405,32 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
   for (int j = 0; j < RY; ++j) {
     const int y = y0 + warp * RY + j;
     if (y >= p.H) continue;
+    CT v[RX];
 #pragma unroll
     for (int i = 0; i < RX; ++i) {
-      const int x = x0 + lane * RX + i;
+      v[i] = acc[j][i];
+      if constexpr (kPackedAbs) v[i] = (j & 1) ? accr[j / 2][i].y : accr[j / 2][i].x;
+      if (kNorm) v[i] = dv(v[i], sq(mul(acc2[j][i], tt)));
+    }
+    char* o = p.dst + (size_t)y * p.dst_pitch;
+    const int xl = x0 + lane * RX;
+    float* of = reinterpret_cast<float*>(o) + (size_t)xl;
+    if (!p.dst_f64 && p.dst_nch == 1 && xl + RX <= p.W && (reinterpret_cast<size_t>(of) & 15) == 0) {
+      // One-channel F32 row segment: 16-byte stores.
+#pragma unroll
+      for (int i = 0; i < RX; i += 4)
+        *reinterpret_cast<float4*>(of + i) =
+            make_float4((float)v[i], (float)v[i + 1], (float)v[i + 2], (float)v[i + 3]);
+      continue;
+    }
+#pragma unroll
+    for (int i = 0; i < RX; ++i) {
+      const int x = xl + i;
       if (x >= p.W) continue;
-      CT v = acc[j][i];
-      if constexpr (kPackedAbs) v = (j & 1) ? accr[j / 2][i].y : accr[j / 2][i].x;
-      if (kNorm) v = dv(v, sq(mul(acc2[j][i], tt)));
-      char* o = p.dst + (size_t)y * p.dst_pitch;
       if (p.dst_f64)
-        reinterpret_cast<double*>(o)[(size_t)x * p.dst_nch + c] = (double)v;
+        reinterpret_cast<double*>(o)[(size_t)x * p.dst_nch + c] = (double)v[i];
       else
-        reinterpret_cast<float*>(o)[(size_t)x * p.dst_nch + c] = (float)v;
+        reinterpret_cast<float*>(o)[(size_t)x * p.dst_nch + c] = (float)v[i];
     }
   }
 }
