@@ -25,10 +25,9 @@
 // every 8, so the lanes' stride-2 (float) or stride-4 (double) chunk accesses
 // hit distinct banks. Very tall templates are processed in row bands.
 //
-// F32 AbsDistance, the one measure without a tensor-core form, runs on
-// sm_100's packed FP32 adds over pairs of output rows (PackedAbs below),
-// specialised on the width of the template's last column chunk so that the
-// inner loop has no bounds tests.
+// F32 sources run on sm_100's packed FP32 arithmetic over pairs of output
+// rows (PackedRows below), specialised on the width of the template's last
+// column chunk so that the inner loop has no bounds tests.
 #include <algorithm>
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -101,19 +100,77 @@ __host__ __device__ inline int row_bytes_for(int L) {
   return (chunks + chunks / 8 + 1) * 16;
 }
 
-// Packed FP32 AbsDistance. Output rows 2jp and 2jp + 1 of one column meet
-// the same source element at every step (their template rows are h and
-// h - 1), so the template is staged as negated row pairs (-t(h, w),
-// -t(h - 1, w)) and one sm_100 packed add (__fadd2_rn) forms both rows'
-// differences, s + (-t) being s - t exactly (IEEE subtraction is the addition
-// of the negation); a second packed add folds their absolute values into the
-// two rows' sums. Every per-output operation and its order are the scalar
-// form's, so the results are bit-identical; the packed adds halve the
-// instructions and, unlike scalar adds, load both halves of the FP32 pipe.
+// Packed FP32 form (F32 sources, every measure). Output rows 2jp and
+// 2jp + 1 of one column meet the same source element at every step (their
+// template rows are h and h - 1), so the template is staged as row pairs
+// (t(h, w), t(h - 1, w)) and each packed instruction (__fadd2_rn,
+// __ffma2_rn: per component the same rounding as __fadd_rn, __fmaf_rn) does
+// the two rows' operation of one term: the difference (the template staged
+// negated, s + (-t) being s - t exactly: IEEE subtraction is the addition of
+// the negation), the absolute-value add, the fused multiply-add of the
+// product or of the square, the energy term s*s. Every per-output operation
+// and its order are the scalar form's, so the results are bit-identical; the
+// packed instructions halve the instruction count and, unlike scalar ones,
+// load both halves of the FMA pipe.
 template <int TYPE, int MEAS>
-struct PackedAbs {
-  static constexpr bool value = TYPE == F32 && MEAS == kAbsDistance;
+struct PackedRows {
+  static constexpr bool value = TYPE == F32;
+  // The template is staged negated for the measures that take differences.
+  static constexpr bool neg = MEAS == kAbsDistance || MEAS == kSqrDistance ||
+                              MEAS == kSqrDistanceNorm;
 };
+
+// One chunk of KMAX template columns for a pair of output rows whose template
+// rows both lie inside the template: sd[e] holds window element e in both
+// halves, tp[k] the pair's (possibly negated) template values of column k.
+template <int MEAS, int KMAX>
+__device__ __forceinline__ void pair_chunk(float2 (&acc)[RX], float2 (&acc2)[RX],
+                                           const float2 (&sd)[RX + WCH], const float2 (&tp)[WCH]) {
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+#pragma unroll
+    for (int i = 0; i < RX; ++i) {
+      const float2 s = sd[i + k];
+      if (MEAS == kAbsDistance) {
+        const float2 d = __fadd2_rn(s, tp[k]);
+        acc[i] = __fadd2_rn(acc[i], make_float2(fabsf(d.x), fabsf(d.y)));
+      } else if (MEAS == kSqrDistance || MEAS == kSqrDistanceNorm) {
+        const float2 d = __fadd2_rn(s, tp[k]);
+        acc[i] = __ffma2_rn(d, d, acc[i]);
+        if (MEAS == kSqrDistanceNorm) acc2[i] = __ffma2_rn(s, s, acc2[i]);
+      } else {
+        acc[i] = __ffma2_rn(s, tp[k], acc[i]);
+        if (MEAS == kCrossCorrNorm) acc2[i] = __ffma2_rn(s, s, acc2[i]);
+      }
+    }
+  }
+}
+
+// The same for one row of the pair (H = 0: row 2jp, the .x halves; H = 1: row
+// 2jp + 1, the .y halves) when the other row's template row lies outside.
+template <int MEAS, int KMAX, int H>
+__device__ __forceinline__ void half_chunk(float2 (&acc)[RX], float2 (&acc2)[RX],
+                                           const float (&win)[RX + WCH], const float (&tv)[WCH]) {
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+#pragma unroll
+    for (int i = 0; i < RX; ++i) {
+      const float s = win[i + k];
+      float& a = H ? acc[i].y : acc[i].x;
+      float& a2 = H ? acc2[i].y : acc2[i].x;
+      if (MEAS == kAbsDistance) {
+        a = __fadd_rn(a, fabsf(__fadd_rn(s, tv[k])));
+      } else if (MEAS == kSqrDistance || MEAS == kSqrDistanceNorm) {
+        const float d = __fadd_rn(s, tv[k]);
+        a = __fmaf_rn(d, d, a);
+        if (MEAS == kSqrDistanceNorm) a2 = __fmaf_rn(s, s, a2);
+      } else {
+        a = __fmaf_rn(s, tv[k], a);
+        if (MEAS == kCrossCorrNorm) a2 = __fmaf_rn(s, s, a2);
+      }
+    }
+  }
+}
 
 // One template-column chunk applied to one output row.
 template <typename CT, int MEAS>
@@ -147,14 +204,14 @@ __device__ __forceinline__ void apply_chunk(CT (&acc)[RX], CT (&acc2)[RX],
   }
 }
 
-// KT: for the packed FP32 AbsDistance form, the columns of the template's last
-// chunk, tw - WCH * ((tw - 1) / WCH), in 1 .. WCH; 0 for the other forms.
+// KT: for the packed FP32 form, the columns of the template's last chunk,
+// tw - WCH * ((tw - 1) / WCH), in 1 .. WCH; 0 for the other forms.
 template <int TYPE, typename CT, int MEAS, int RY, int KT>
 __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     prox_plain_kernel(const PlainParams p) {
   using ET = typename ElemOf<TYPE>::T;
   constexpr bool kNorm = (MEAS == kCrossCorrNorm || MEAS == kSqrDistanceNorm);
-  constexpr bool kPackedAbs = PackedAbs<TYPE, MEAS>::value;
+  constexpr bool kPacked = PackedRows<TYPE, MEAS>::value;
   constexpr int TY = kWarps * RY;
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* s_src = smem;
@@ -170,15 +227,19 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
   const int L = TX + p.twp;          // logical elements per source row
   const int qtot = TY + p.th - 1;    // source rows needed by the tile
   const int nwc = p.twp / WCH;
-  const int tstride = kPackedAbs ? 2 * p.twp : p.twp;  // template row stride in s_t
+  const int tstride = kPacked ? 2 * p.twp : p.twp;  // template row stride in s_t
 
   CT acc[RY][RX];
   CT acc2[RY][RX];
-  float2 accr[RY / 2][RX];  // packed AbsDistance: output rows (2jp, 2jp + 1) of column i
+  // Packed form: output rows (2jp, 2jp + 1) of column i.
+  float2 accr[RY / 2][RX], accr2[RY / 2][RX];
 #pragma unroll
   for (int j = 0; j < RY / 2; ++j)
 #pragma unroll
-    for (int i = 0; i < RX; ++i) accr[j][i] = make_float2(0.f, 0.f);
+    for (int i = 0; i < RX; ++i) {
+      accr[j][i] = make_float2(0.f, 0.f);
+      accr2[j][i] = make_float2(0.f, 0.f);
+    }
 #pragma unroll
   for (int j = 0; j < RY; ++j)
 #pragma unroll
@@ -228,7 +289,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     }
     if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.commit_group;\n" ::: "memory");
     // Stage template rows [tg0, tg1), zero-padded to twp columns. The packed
-    // AbsDistance form stores row h as the negated pairs (t(h, w), t(h - 1, w)).
+    // form stores row h as the pairs (t(h, w), t(h - 1, w)), negated for the
+    // measures that take differences.
     // Read-only loads, unrolled, so that a thread's loads are in flight together.
     const int ntel = (tg1 - tg0) * tstride;
 #pragma unroll 8
@@ -236,7 +298,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
       const int hh = idx / tstride;
       int w = idx - hh * tstride;
       int trow = tg0 + hh;
-      if (kPackedAbs) {  // pairs (row h, row h - 1) of column w
+      if (kPacked) {  // pairs (row h, row h - 1) of column w
         w = (idx - hh * tstride) >> 1;
         trow -= (idx - hh * tstride) & 1;
       }
@@ -244,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
       if (w < p.tw && trow >= 0)
         v = (CT)__ldg(reinterpret_cast<const ET*>(
             p.tmpl + (size_t)trow * p.tmpl_pitch + ((size_t)w * p.nch + c) * sizeof(ET)));
-      s_t[idx] = kPackedAbs ? -v : v;
+      s_t[idx] = (kPacked && PackedRows<TYPE, MEAS>::neg) ? -v : v;
     }
     if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
@@ -313,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
         }
       }
     };
-    if constexpr (kPackedAbs) {
+    if constexpr (kPacked) {
       // Chunks of WCH template columns: nfull full ones, then the last, of
       // KT columns. check: some of the rows' template rows may lie outside.
       const int nfull = (p.tw - 1) / WCH;
@@ -341,21 +403,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
               if (both == 3) {
                 const float4* tr =
                     reinterpret_cast<const float4*>(t0 - (size_t)(2 * jp) * tstride + 2 * wc * WCH);
-                float2 tp[WCH];  // (-t(h, k), -t(h - 1, k)), h the template row of output row 2jp
+                float2 tp[WCH];  // (t(h, k), t(h - 1, k)), h the template row of output row 2jp
 #pragma unroll
                 for (int m = 0; m < WCH / 2; ++m) {
                   const float4 f = tr[m];
                   tp[2 * m] = make_float2(f.x, f.y);
                   tp[2 * m + 1] = make_float2(f.z, f.w);
                 }
-#pragma unroll
-                for (int k = 0; k < KMAX; ++k) {
-#pragma unroll
-                  for (int i = 0; i < RX; ++i) {
-                    const float2 d = __fadd2_rn(sd[i + k], tp[k]);
-                    accr[jp][i] = __fadd2_rn(accr[jp][i], make_float2(fabsf(d.x), fabsf(d.y)));
-                  }
-                }
+                pair_chunk<MEAS, KMAX>(accr[jp], accr2[jp], sd, tp);
               } else if (both != 0) {
                 // The one template row inside: h (output row 2jp) or h - 1
                 // (row 2jp + 1), read from its own staged row.
@@ -368,19 +423,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
                   tv[2 * m] = f.x;
                   tv[2 * m + 1] = f.z;
                 }
-                if (both == 1) {
-#pragma unroll
-                  for (int k = 0; k < KMAX; ++k)
-#pragma unroll
-                    for (int i = 0; i < RX; ++i)
-                      accr[jp][i].x = __fadd_rn(accr[jp][i].x, fabsf(__fadd_rn(win[i + k], tv[k])));
-                } else {
-#pragma unroll
-                  for (int k = 0; k < KMAX; ++k)
-#pragma unroll
-                    for (int i = 0; i < RX; ++i)
-                      accr[jp][i].y = __fadd_rn(accr[jp][i].y, fabsf(__fadd_rn(win[i + k], tv[k])));
-                }
+                if (both == 1)
+                  half_chunk<MEAS, KMAX, 0>(accr[jp], accr2[jp], win, tv);
+                else
+                  half_chunk<MEAS, KMAX, 1>(accr[jp], accr2[jp], win, tv);
               }
             }
           };
@@ -409,8 +455,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
 #pragma unroll
     for (int i = 0; i < RX; ++i) {
       v[i] = acc[j][i];
-      if constexpr (kPackedAbs) v[i] = (j & 1) ? accr[j / 2][i].y : accr[j / 2][i].x;
-      if (kNorm) v[i] = dv(v[i], sq(mul(acc2[j][i], tt)));
+      CT e2 = acc2[j][i];
+      if constexpr (kPacked) {
+        v[i] = (j & 1) ? accr[j / 2][i].y : accr[j / 2][i].x;
+        e2 = (j & 1) ? accr2[j / 2][i].y : accr2[j / 2][i].x;
+      }
+      if (kNorm) v[i] = dv(v[i], sq(mul(e2, tt)));
     }
     char* o = p.dst + (size_t)y * p.dst_pitch;
     const int xl = x0 + lane * RX;
@@ -494,7 +544,7 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
   auto bytes_for = [&](int rb) {
     const int tb = std::min(p.th, rb + TY - 1);
     return (size_t)rb * p.rowBytes +
-           (size_t)tb * p.twp * sizeof(CT) * (PackedAbs<TYPE, MEAS>::value ? 2 : 1);
+           (size_t)tb * p.twp * sizeof(CT) * (PackedRows<TYPE, MEAS>::value ? 2 : 1);
   };
   while (RB > 1 && bytes_for(RB) > (size_t)kSmemBudget) RB = (RB + 1) / 2;
   if (bytes_for(RB) > (size_t)kSmemBudget) return cudaErrorInvalidValue;
@@ -509,8 +559,8 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
         (const char*)tmpl.ptr, tmpl.pitch, tmpl.nch, p.tw, p.th, (CT*)tt_buf);
     count_launches(1);
   }
-  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY, PackedAbs<TYPE, MEAS>::value ? WCH : 0>;
-  if constexpr (PackedAbs<TYPE, MEAS>::value) {
+  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY, PackedRows<TYPE, MEAS>::value ? WCH : 0>;
+  if constexpr (PackedRows<TYPE, MEAS>::value) {
     switch (p.tw - WCH * ((p.tw - 1) / WCH)) {
       case 1: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 1>; break;
       case 2: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 2>; break;
