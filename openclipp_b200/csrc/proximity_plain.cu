@@ -25,9 +25,9 @@
 // every 8, so the lanes' stride-2 (float) or stride-4 (double) chunk accesses
 // hit distinct banks. Very tall templates are processed in row bands.
 //
-// F32 sources run on sm_100's packed FP32 arithmetic over pairs of output
-// rows (PackedRows below), specialised on the width of the template's last
-// column chunk so that the inner loop has no bounds tests.
+// FP32 compute types run on sm_100's packed FP32 arithmetic over pairs of
+// output rows (PackedRows below), specialised on the width of the template's
+// last column chunk so that the inner loop has no bounds tests.
 #include <algorithm>
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -100,7 +100,7 @@ __host__ __device__ inline int row_bytes_for(int L) {
   return (chunks + chunks / 8 + 1) * 16;
 }
 
-// Packed FP32 form (F32 sources, every measure). Output rows 2jp and
+// Packed FP32 form (every measure, FP32 compute type). Output rows 2jp and
 // 2jp + 1 of one column meet the same source element at every step (their
 // template rows are h and h - 1), so the template is staged as row pairs
 // (t(h, w), t(h - 1, w)) and each packed instruction (__fadd2_rn,
@@ -112,9 +112,11 @@ __host__ __device__ inline int row_bytes_for(int L) {
 // and its order are the scalar form's, so the results are bit-identical; the
 // packed instructions halve the instruction count and, unlike scalar ones,
 // load both halves of the FMA pipe.
-template <int TYPE, int MEAS>
+template <typename CT, int MEAS>
 struct PackedRows {
-  static constexpr bool value = TYPE == F32;
+  // FP32 compute type: F32 sources, and 8-bit ones whose sums are exact in
+  // float (integer arithmetic, so any order gives the same values).
+  static constexpr bool value = std::is_same<CT, float>::value;
   // The template is staged negated for the measures that take differences.
   static constexpr bool neg = MEAS == kAbsDistance || MEAS == kSqrDistance ||
                               MEAS == kSqrDistanceNorm;
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
     prox_plain_kernel(const PlainParams p) {
   using ET = typename ElemOf<TYPE>::T;
   constexpr bool kNorm = (MEAS == kCrossCorrNorm || MEAS == kSqrDistanceNorm);
-  constexpr bool kPacked = PackedRows<TYPE, MEAS>::value;
+  constexpr bool kPacked = PackedRows<CT, MEAS>::value;
   constexpr int TY = kWarps * RY;
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned char* s_src = smem;
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(CT) == 4 ? 2 : 1)
       if (w < p.tw && trow >= 0)
         v = (CT)__ldg(reinterpret_cast<const ET*>(
             p.tmpl + (size_t)trow * p.tmpl_pitch + ((size_t)w * p.nch + c) * sizeof(ET)));
-      s_t[idx] = (kPacked && PackedRows<TYPE, MEAS>::neg) ? -v : v;
+      s_t[idx] = (kPacked && PackedRows<CT, MEAS>::neg) ? -v : v;
     }
     if constexpr (std::is_same<CT, ET>::value) asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
@@ -544,7 +546,7 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
   auto bytes_for = [&](int rb) {
     const int tb = std::min(p.th, rb + TY - 1);
     return (size_t)rb * p.rowBytes +
-           (size_t)tb * p.twp * sizeof(CT) * (PackedRows<TYPE, MEAS>::value ? 2 : 1);
+           (size_t)tb * p.twp * sizeof(CT) * (PackedRows<CT, MEAS>::value ? 2 : 1);
   };
   while (RB > 1 && bytes_for(RB) > (size_t)kSmemBudget) RB = (RB + 1) / 2;
   if (bytes_for(RB) > (size_t)kSmemBudget) return cudaErrorInvalidValue;
@@ -559,8 +561,8 @@ cudaError_t launch_typed(const DevImage& src, const DevImage& tmpl,
         (const char*)tmpl.ptr, tmpl.pitch, tmpl.nch, p.tw, p.th, (CT*)tt_buf);
     count_launches(1);
   }
-  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY, PackedRows<TYPE, MEAS>::value ? WCH : 0>;
-  if constexpr (PackedRows<TYPE, MEAS>::value) {
+  auto kern = prox_plain_kernel<TYPE, CT, MEAS, RY, PackedRows<CT, MEAS>::value ? WCH : 0>;
+  if constexpr (PackedRows<CT, MEAS>::value) {
     switch (p.tw - WCH * ((p.tw - 1) / WCH)) {
       case 1: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 1>; break;
       case 2: kern = prox_plain_kernel<TYPE, CT, MEAS, RY, 2>; break;
