@@ -1195,6 +1195,36 @@ def run_integral_bench(args, world, rank, local):
     return result
 
 
+def side_workloads(args, world, rank, local):
+    """Short runs of the other workloads beside the headline (batch, backward,
+    integral, sad), so that one default run records each of them: 5 timed
+    steps after 3 warm-up steps, no CPU baselines, each with its own checks
+    against the oracle. A workload that fails records its error instead of
+    ending the run."""
+    import copy
+    import gc
+
+    import torch
+
+    out = {}
+    for name, fn in (("batch", run_batch_bench), ("backward", run_backward_bench),
+                     ("integral", run_integral_bench), ("sad", run_sad_bench)):
+        a = copy.copy(args)
+        a.steps, a.warmup, a.no_cpu_baseline = 5, 3, True
+        t0 = time.time()
+        try:
+            r = fn(a, world, rank, local)
+            r = {k: v for k, v in r.items() if k not in ("n_gpus", "higher_is_better", "scaling",
+                                                         "vs_baseline", "cpu_baseline")}
+        except Exception as e:  # recorded, so that the headline line still prints
+            r = {"error": f"{type(e).__name__}: {e}"}
+        r["wall_s"] = round(time.time() - t0, 1)
+        out[name] = r
+        gc.collect()
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1209,6 +1239,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm (profiling)")
     ap.add_argument("--no-plain-arm", action="store_true",
                     help="skip timing the plain FP32 kernels beside the tensor path (profiling)")
+    ap.add_argument("--no-side-workloads", action="store_true",
+                    help="skip the short runs of the batch, backward, integral and sad "
+                         "workloads that a default single-GPU run adds to its line")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the error reports against the oracle (profiling)")
     ap.add_argument("--workload", choices=["single", "batch", "backward", "integral", "sad"],
@@ -1240,6 +1273,8 @@ def main():
         res = run_sad_bench(args, world, rank, local)
     else:
         res = run_ours(args, world, rank, local)
+        if world == 1 and not args.no_side_workloads:
+            res["side_workloads"] = side_workloads(args, world, rank, local)
     if rank == 0:
         print(json.dumps(res))
     import torch.distributed as dist
