@@ -170,6 +170,23 @@ ocipError ocip_API ocipTestBoundedWait(int LimitCycles);
 ocipError ocip_API ocipGetImageDevicePtr(ocipImage Image, void** DevicePtr,
                                          size_t* Pitch);
 
+/* Row band of one image that part Part of Parts computes when the
+ * ImageProximity calls of an image of Height rows and a template of
+ * TemplateHeight rows are split across GPUs (one context per GPU; no
+ * counterpart in the reference, whose contexts never share an image).
+ * Rows[0] .. Rows[1] (exclusive) are the destination rows the part owns: the
+ * image's rows split as evenly as possible, in order. Rows[2] .. Rows[3] are
+ * the source rows it needs: its own rows shifted by the template anchor
+ * (TemplateHeight / 2) plus a halo of TemplateHeight - 1 rows, clipped to the
+ * image and, near its edges, widened to at least TemplateHeight rows (the
+ * measures refuse a source shorter than the template). Running a measure on the image made of those source rows gives, at
+ * its rows Rows[0] - Rows[2] .. Rows[1] - Rows[2], the same values as the
+ * whole image gives at rows Rows[0] .. Rows[1]: the zero padding then falls
+ * only outside the whole image. A part may own no rows (Parts > Height); its
+ * source band is then empty too. Host arithmetic only: needs no context. */
+ocipError ocip_API ocipGetProximityBand(unsigned int Height, unsigned int TemplateHeight,
+                                        int Part, int Parts, unsigned int Rows[4]);
+
 #ifdef __cplusplus
 }
 #endif

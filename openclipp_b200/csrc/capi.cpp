@@ -423,4 +423,37 @@ ocipError ocipGetImageDevicePtr(ocipImage h, void** DevicePtr, size_t* Pitch) {
   )
 }
 
+ocipError ocipGetProximityBand(unsigned int Height, unsigned int TemplateHeight, int Part,
+                               int Parts, unsigned int Rows[4]) {
+  if (Rows == nullptr || Parts < 1 || Part < 0 || Part >= Parts || TemplateHeight == 0 ||
+      TemplateHeight > Height)
+    return CL_INVALID_VALUE;
+  // Owned rows: the first Height % Parts parts take one row more.
+  const uint64_t base = Height / (unsigned)Parts, extra = Height % (unsigned)Parts;
+  const uint64_t p = (uint64_t)Part;
+  const uint64_t y0 = p * base + (p < extra ? p : extra);
+  const uint64_t y1 = y0 + base + (p < extra ? 1 : 0);
+  Rows[0] = (unsigned)y0;
+  Rows[1] = (unsigned)y1;
+  if (y1 == y0) {
+    Rows[2] = Rows[3] = (unsigned)y0;
+    return CL_SUCCESS;
+  }
+  // Destination row y reads source rows y - ay .. y - ay + th - 1.
+  const int64_t ay = TemplateHeight / 2;
+  const int64_t s0 = (int64_t)y0 - ay;
+  const int64_t s1 = (int64_t)y1 - ay + TemplateHeight - 1;
+  int64_t a = s0 < 0 ? 0 : s0, b = s1 > (int64_t)Height ? (int64_t)Height : s1;
+  // Near an edge the clipped band can be shorter than the template; widen it
+  // with real rows (which change none of the owned outputs) to pass the
+  // template-size check of the measure calls.
+  if (b - a < (int64_t)TemplateHeight) {
+    if (a == 0) b = TemplateHeight;
+    else a = b - (int64_t)TemplateHeight;
+  }
+  Rows[2] = (unsigned)a;
+  Rows[3] = (unsigned)b;
+  return CL_SUCCESS;
+}
+
 }  // extern "C"

@@ -115,6 +115,8 @@ def _load():
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "ocipMaxAbsIndx": (i32, [vp, vp, ctypes.POINTER(ctypes.c_double),
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+        "ocipGetProximityBand": (i32, [u32, u32, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(u32)]),
         "ocipGetProximityBatchInfo": (i32, [vp, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
