@@ -500,6 +500,8 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
       const uint32_t a0 = smem_u32(smem + L.a);
       const uint32_t b0 = smem_u32(smem + L.b);
       const uint32_t bstride = G.NB * 16;  // between B core matrices
+      const uint32_t dhi = desc_hi(128);     // every descriptor: SBO 128 bytes
+      const uint32_t astep = G.lbok >> 4, bstep = (2 * bstride) >> 4;  // 16-byte units
       int i = 0;
       uint32_t ph = 0;
       for (int t = 0; t < nsteps; ++t) {
@@ -515,18 +517,33 @@ __device__ __forceinline__ void run_item(const ItemArgs& a, unsigned char* smem,
         const uint32_t bq = b0 + 16 * S * (Q - 1 - q);
         // The block's first MMA overwrites all kNp columns of the partial.
         const uint32_t acc0 = q == 0 ? 0u : 1u;
+        // Descriptors advance by one add of their low word per MMA: B by two
+        // core matrices, A by one (split, hi/lo pairs) or two K core matrices.
+        // The MMAs of a step issue back to back from this one thread, so the
+        // work between two of them delays the tensor pipe directly.
+        uint32_t bl = desc_lo(bq, bstride);
         if (SPLIT) {
-          const uint32_t lo_off = G.QR * 16;
-          for (int c = 0; c < G.KC; ++c)
-            mma_bf16(d, smem_desc(ah + c * G.lbok, lo_off, 128),
-                     smem_desc(bq + 2 * c * bstride, bstride, 128), idesc, c == 0 ? acc0 : 1u);
-          for (int j = 0; j < G.nmma - G.KC; ++j)
-            mma_bf16(d, smem_desc(ah + 2 * j * G.lbok, G.lbok, 128),
-                     smem_desc(bq + 2 * (G.KC + j) * bstride, bstride, 128), idesc, 1u);
+          uint32_t al = desc_lo(ah, G.QR * 16), acc = acc0;
+          for (int c = 0; c < G.KC; ++c) {
+            mma_bf16_h(d, al, dhi, bl, dhi, idesc, acc);
+            acc = 1u;
+            al += astep;
+            bl += bstep;
+          }
+          uint32_t al2 = desc_lo(ah, G.lbok);
+          for (int j = G.KC; j < G.nmma; ++j) {
+            mma_bf16_h(d, al2, dhi, bl, dhi, idesc, 1u);
+            al2 += 2 * astep;
+            bl += bstep;
+          }
         } else {
-          for (int j = 0; j < G.nmma; ++j)
-            mma_i8(d, smem_desc(ah + 2 * j * G.lbok, G.lbok, 128),
-                   smem_desc(bq + 2 * j * bstride, bstride, 128), idesc, j == 0 ? acc0 : 1u);
+          uint32_t al = desc_lo(ah, G.lbok), acc = acc0;
+          for (int j = 0; j < G.nmma; ++j) {
+            mma_i8_h(d, al, dhi, bl, dhi, idesc, acc);
+            acc = 1u;
+            al += 2 * astep;
+            bl += bstep;
+          }
         }
         // One commit per block: it frees the block's partial for the epilogue
         // and its A stages for the builders.

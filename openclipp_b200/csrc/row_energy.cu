@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <cstring>
 #include <type_traits>
 
 #include "internal.h"
@@ -116,9 +118,97 @@ __global__ void __launch_bounds__(kWarps * 32) row_energy_kernel(const RowEnergy
   }
 }
 
+// One-channel form: the segment's source pixels are staged raw with 16-byte
+// loads (from the 16-byte group at or below its first pixel, so `sh` pixels
+// lead), squared and prefix-summed in registers, and only the prefix sums
+// are written back for the differences. Same sums, in the same order, as
+// row_energy_kernel.
+template <typename ET, int K>
+__global__ void __launch_bounds__(kWarps * 32) row_energy_vec_kernel(const RowEnergyParams p) {
+  typedef typename RowSumOf<ET>::A A;
+  typedef typename RowSumOf<ET>::R RT;
+  constexpr int kInner = 16 / (int)sizeof(ET);                      // pixels per group
+  constexpr int kRawGroups = (32 * K + kInner - 1) / kInner + 1;     // covers sh + 32 K
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.y * kWarps + warp;
+  if (r >= p.H) return;  // whole warp
+  const int x0 = blockIdx.x * kSeg;
+  A* buf = reinterpret_cast<A*>(smem) + warp * (32 * K);
+  ET* raw = reinterpret_cast<ET*>(smem + (size_t)kWarps * 32 * K * sizeof(A)) +
+            warp * (kRawGroups * kInner);
+  const ET* row = reinterpret_cast<const ET*>(p.src + (size_t)r * p.src_pitch);
+  const int n = kSeg + p.tw - 1;
+  const int xs0 = x0 - p.ax;
+  const int xa = xs0 >= 0 ? xs0 - xs0 % kInner : -((-xs0 + kInner - 1) / kInner) * kInner;
+  const int sh = xs0 - xa;
+  // Raw pixels xa .. xa + kRawGroups * kInner - 1, zero outside the image:
+  // whole groups inside the row with one 16-byte load, the rest per pixel.
+  for (int g = lane; g < kRawGroups; g += 32) {
+    const int x = xa + g * kInner;
+    uint4 v;
+    if (x >= 0 && x + kInner <= p.W) {
+      v = __ldg(reinterpret_cast<const uint4*>(row + x));
+    } else {
+      ET e[kInner];
+#pragma unroll
+      for (int i = 0; i < kInner; ++i) e[i] = (x + i >= 0 && x + i < p.W) ? row[x + i] : ET(0);
+      memcpy(&v, e, sizeof(v));
+    }
+    reinterpret_cast<uint4*>(raw)[g] = v;
+  }
+  __syncwarp();
+  // Lane l: staged entries K l .. K l + K - 1 (pixel xs0 + i is raw[sh + i]).
+  A loc[K];
+  A tot = A(0);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i = K * lane + k;
+    const A e = i < n ? static_cast<A>(raw[sh + i]) : A(0);
+    tot += e * e;
+    loc[k] = tot;
+  }
+  A incl = tot;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const A o = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += o;
+  }
+  const A excl = incl - tot;
+#pragma unroll
+  for (int k = 0; k < K; ++k) buf[K * lane + k] = excl + loc[k];
+  __syncwarp();
+  RT* dst = reinterpret_cast<RT*>(p.dst + (size_t)r * p.dst_pitch);
+#pragma unroll
+  for (int u = 0; u < kSeg / 32; ++u) {
+    const int j = lane + 32 * u;
+    const int x = x0 + j;
+    if (x < p.W) {
+      const A hi = buf[j + p.tw - 1];
+      const A lo = j > 0 ? buf[j - 1] : A(0);
+      dst[x] = static_cast<RT>(hi - lo);
+    }
+  }
+}
+
 template <typename ET, int K>
 cudaError_t launch_k(const RowEnergyParams& p, cudaStream_t st) {
   typedef typename RowSumOf<ET>::A A;
+  if (p.nch == 1 && (p.src_pitch % 16) == 0 && ((uintptr_t)p.src % 16) == 0) {
+    constexpr int kInner = 16 / (int)sizeof(ET);
+    constexpr int kRawGroups = (32 * K + kInner - 1) / kInner + 1;
+    const size_t smem = (size_t)kWarps * (32 * K * sizeof(A) + kRawGroups * 16);
+    auto kern = row_energy_vec_kernel<ET, K>;
+    if (smem > 48 * 1024) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    dim3 grid((p.W + kSeg - 1) / kSeg, (p.H + kWarps - 1) / kWarps, 1);
+    kern<<<grid, kWarps * 32, smem, st>>>(p);
+    count_launches(1);
+    return cudaGetLastError();
+  }
   const size_t smem = (size_t)kWarps * 32 * K * sizeof(A);
   auto kern = row_energy_kernel<ET, K>;
   if (smem > 48 * 1024) {

@@ -303,6 +303,42 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
+// The halves of smem_desc(saddr, lbo, sbo): the low word holds the start
+// address and LBO fields, the high word SBO and the version bit. Adding
+// n to the low word moves the start address by 16 n bytes (shared addresses
+// stay below 2^18, so the 14-bit field never carries into LBO).
+__device__ __forceinline__ uint32_t desc_lo(uint32_t saddr, uint32_t lbo) {
+  return ((saddr >> 4) & 0x3FFFu) | (((lbo >> 4) & 0x3FFFu) << 16);
+}
+__device__ __forceinline__ uint32_t desc_hi(uint32_t sbo) {
+  return ((sbo >> 4) & 0x3FFFu) | (1u << 14);
+}
+
+// mma_bf16 / mma_i8 with each descriptor given as its two halves, so that a
+// chain of MMAs advances a descriptor with one 32-bit add.
+__device__ __forceinline__ void mma_bf16_h(uint32_t d, uint32_t alo, uint32_t ahi, uint32_t blo,
+                                           uint32_t bhi, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t.reg .b64 da, db;\n\t"
+      "setp.ne.b32 p, %6, 0;\n\t"
+      "mov.b64 da, {%1, %2};\n\t"
+      "mov.b64 db, {%3, %4};\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, p;\n\t}" ::"r"(d),
+      "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_i8_h(uint32_t d, uint32_t alo, uint32_t ahi, uint32_t blo,
+                                         uint32_t bhi, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t.reg .b64 da, db;\n\t"
+      "setp.ne.b32 p, %6, 0;\n\t"
+      "mov.b64 da, {%1, %2};\n\t"
+      "mov.b64 db, {%3, %4};\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], da, db, %5, p;\n\t}" ::"r"(d),
+      "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Instruction descriptors (32-bit): D format [4,6), A format [7,10),
 // B format [10,13), A/B major [15], [16] (0 = K-major), N>>3 [17,23),
 // M>>4 [24,29).
