@@ -61,6 +61,16 @@ def test_u8_tensor_equals_plain(ocip, ctx, th, tw):
         tens, p2 = run(ocip, ctx, m, S, T, ocip.PATH_TENSOR)
         assert p1 == ocip.PATH_PLAIN and p2 == ocip.PATH_TENSOR
         assert np.array_equal(plain, tens, equal_nan=True), MEAS[m]
+        # and against the exact oracle directly: integer scores bit-exact, the
+        # _Norm ratios within 2 FP32 rounding units of the exact value
+        ex = O.proximity_exact(m, S, T)
+        if m in (0, 3):
+            assert np.array_equal(tens, ex.astype(np.float32)), MEAS[m]
+        else:
+            fin = np.isfinite(ex) & (ex != 0)
+            assert np.array_equal(np.isnan(tens), np.isnan(ex.astype(np.float32))), MEAS[m]
+            rel = np.abs(tens[fin].astype(np.float64) - ex[fin]) / np.abs(ex[fin])
+            assert rel.max() <= 2.0 ** -22, MEAS[m]
     ctx.set_path(ocip.PATH_PLAIN)
 
 
